@@ -1,0 +1,296 @@
+"""Benchmark: Mcells/s of receivers -> carve reroute -> accumulate on one DEM.
+
+Workload (default): 4096 x 4096 float32 DEM from the seeded spectral generator
+(relief 0-1500 m, 2000 Gaussian pits), periodic east-west with outlets on the
+north and south rows, carve rerouting on, accumulation of exact uint32 counts and
+lognormal(0, 0.5) precipitation-weighted discharge in one pass.
+
+A step = FlowRouter.compute_receivers -> reroute_flow -> accumulate_weighted_Q
+on the resident DEM.  value = cells x steps / device time (CUDA events, L2
+flushed between steps).  e2e = the same chain through the public API with the
+DEM and weights copied from pinned host memory and Q + counts copied back, every
+step, inside the timed region.
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference itself is Python on Taichi, which is not installable here) on a
+bounded sample of the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcells/s route+reroute+accumulate"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# algorithmic bytes per cell (z in, rcv+gradient out | rcv+z in, rcv+bid out | rcv+w in, Q+counts out)
+ALG_BYTES = {"receivers": 12, "reroute": 16, "accumulate": 16}
+
+
+def peak_hbm():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(n, seed=2):
+    from pyfastflow_b200 import synthetic
+
+    cache = os.path.join(tempfile.gettempdir(), f"pff_routing_lakes_{n}_{seed}.npz")
+    if os.path.exists(cache):
+        d = np.load(cache)
+        return d["z"], d["w"]
+    w = synthetic.routing_lakes(n, seed=seed)
+    wt = synthetic.lognormal_weights(n * n, seed + 100)
+    try:
+        np.savez(cache, z=w["z"], w=wt)
+    except OSError:
+        pass
+    return w["z"], wt
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def run_cpu_reference(z, w, n, threads):
+    """The CPU restatement of the reference chain (oracle) on one DEM; returns seconds."""
+    from oracle import oracle as O
+
+    g = O.Grid(n, n, 1)
+    t0 = time.perf_counter()
+    rcv, _ = O.compute_receivers(z, g, 30.0)
+    r2, _, _, _, _ = O.reroute_flow(rcv, z, g, carve=True)
+    O.accumulate(r2, w, with_counts=True)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(threads):
+    from oracle import oracle as O
+
+    O.build()
+    used = O.set_threads(threads)
+    n = 1024
+    z, w = workload(n, seed=2)
+    return n, z, w, used
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = args.size
+    cfg = {"workload": f"routing_lakes {n}x{n} f32 DEM, relief 0-1500 m, 2000 pits per 4096^2, periodic EW, "
+                       "carve reroute, uint32 counts + lognormal(0,0.5) weighted Q",
+           "cells": n * n, "dx": 30.0, "boundary": "periodic_EW", "l2": "flushed between steps (256 MiB write)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        sn, z, w, used = cpu_sample(threads)
+        for _ in range(args.warmup):
+            run_cpu_reference(z, w, sn, used)
+        ts = [run_cpu_reference(z, w, sn, used) for _ in range(args.steps)]
+        tot = sum(ts)
+        v = sn * sn * args.steps / tot / 1e6
+        sample = f"{sn}x{sn} DEM of the same generator per step (1/{(n // sn) ** 2} of the cells)"
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "Mcells/s", "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": "Mcells/s", "cores": used, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": v, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    import pyfastflow_b200 as pf
+    from pyfastflow_b200 import _lib
+
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _lib.load()
+
+    z, w = workload(n)
+    router = pf.flow.FlowRouter(n, n, 30.0, boundary_mode="periodic_EW", device=dev)
+    router.set_z(z)
+    wd = torch.from_numpy(w).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        router.compute_receivers()
+        router.reroute_flow()
+        router.accumulate_weighted_Q(wd)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed value ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    l0 = lib.pff_launch_count()
+    with Clocks(torch.cuda.current_device()) as clk:
+        barrier()
+        for s in range(args.steps):
+            flush.fill_(s & 0xFF)
+            ev[s][0].record()
+            step()
+            ev[s][1].record()
+        barrier()
+    launches = (lib.pff_launch_count() - l0) // args.steps
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    t_dev = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t_dev, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t_dev.item())
+    value = world * n * n * args.steps / (ms * 1e-3) / 1e6
+
+    # ---- per-stage times (separate pass) -> roofline of the dominant stage ----
+    stages = {"receivers": [], "reroute": [], "accumulate": []}
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        router.compute_receivers()
+        e[1].record()
+        router.reroute_flow()
+        e[2].record()
+        router.accumulate_weighted_Q(wd)
+        e[3].record()
+        torch.cuda.synchronize()
+        for k, name in enumerate(stages):
+            stages[name].append(e[k].elapsed_time(e[k + 1]))
+    st_ms = {k: sum(v) / len(v) for k, v in stages.items()}
+    dom = max(st_ms, key=st_ms.get)
+    pk, pk_kind = peak_hbm()
+    ach = ALG_BYTES[dom] * n * n / (st_ms[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
+                "peak_source": pk_kind, "traffic": None,
+                "alg_bytes_per_cell": ALG_BYTES[dom], "stage_ms": st_ms}
+
+    # ---- e2e through the public API with host buffers ----
+    zh = torch.from_numpy(z.ravel()).pin_memory()
+    wh = torch.from_numpy(w).pin_memory()
+    qh = torch.empty(n * n, dtype=torch.float32).pin_memory()
+    ch = torch.empty(n * n, dtype=torch.int32).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in range(e2e_steps):
+        router.z.copy_(zh, non_blocking=True)
+        router.Q.copy_(wh, non_blocking=True)
+        router.compute_receivers()
+        router.reroute_flow()
+        router._accumulate(True)
+        qh.copy_(router.Q, non_blocking=True)
+        ch.copy_(router.counts, non_blocking=True)
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    t_e = torch.tensor([e2e_ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t_e, op=torch.distributed.ReduceOp.MAX)
+    e2e_v = world * n * n * e2e_steps / (float(t_e.item()) * 1e-3) / 1e6
+
+    out = {"metric": METRIC, "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded spectral DEM + Gaussian pits)",
+           "config": dict(cfg, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                          n_outer_reroute=router.last_n_outer),
+           "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(launches),
+           "e2e": {"value": e2e_v, "unit": "Mcells/s", "h2d_bytes_per_step": 8 * n * n,
+                   "d2h_bytes_per_step": 8 * n * n, "steps": e2e_steps}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sn, zs, ws, used = cpu_sample(threads)
+        run_cpu_reference(zs, ws, sn, used)
+        ts = [run_cpu_reference(zs, ws, sn, used) for _ in range(2)]
+        out["cpu_baseline"] = {"value": sn * sn * 2 / sum(ts) / 1e6, "unit": "Mcells/s", "cores": used,
+                               "kind": "port",
+                               "sample": f"{sn}x{sn} DEM of the same generator, 2 runs after 1 warm-up"}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+/*
+ * libpff — B200 (sm_100a) flow routing and GraphFlood hot path, C ABI.
+ *
+ * Every entry point takes plain device pointers (CUDA global memory), sizes, and
+ * a CUDA stream (cudaStream_t passed as void*; NULL = legacy default stream).
+ * Nothing here allocates device memory except where a call says so: scratch is a
+ * caller-provided device buffer whose size the matching *_workspace_bytes()
+ * query returns.  Calls are asynchronous on `stream` unless documented as
+ * returning a host-visible count (those synchronize the stream).
+ *
+ * Status: 0 = PFF_OK; on error the call returns a nonzero PFF_ERR_* code and
+ * pff_last_error_string() describes it (per host thread).  No call aborts,
+ * prints or traps.
+ *
+ * Grid arguments restate pyfastflow's compile-time globals (pyfastflow/constants.py:
+ * NX :31, NY :34, DX :28, BOUND_MODE :50, boundaries :53) as runtime values:
+ *   nx, ny      grid columns / rows (nx, ny >= 2), cells are row-major i = row*nx + col
+ *   dx          cell size
+ *   bound_mode  0 normal, 1 periodic east-west, 2 periodic north-south, 3 custom
+ *   codes       N uint8 boundary codes (device), custom mode only, else NULL
+ *               (0 nodata, 1 normal, 3 outlet, 7 inlet, 9 periodic)
+ * Receivers are int32 cell indices; basin arrays (basin_saddle, outlet,
+ * basin_saddlenode) have N+1 entries.
+ */
+#ifndef PFF_H
+#define PFF_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFF_OK 0
+#define PFF_ERR_ARG 1        /* invalid argument (size, pointer, mode) */
+#define PFF_ERR_CUDA 2       /* CUDA runtime error (launch or copy) */
+#define PFF_ERR_NOCONV 3     /* iteration cap reached before convergence */
+#define PFF_ERR_WORKSPACE 4  /* workspace too small */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int pff_version(void);
+/* Description of the last error on the calling host thread ("" if none). */
+const char *pff_last_error_string(void);
+/* Total number of CUDA kernels this library has launched in this process (no
+ * counterpart in the reference: used to report GPU launches per step). */
+long long pff_launch_count(void);
+
+/* ---- receivers --------------------------------------------------------------
+ * Replaces pyfastflow/flow/receivers.py:15-58 compute_receivers(z, receivers,
+ * gradient): D4 steepest descent, strict '>' (first direction k wins ties),
+ * IEEE f32 (z[i]-z[j])/dx; self-receiver for pits and flats. */
+int pff_compute_receivers(const float *z, int32_t *receivers, float *gradient, int nx, int ny,
+                          float dx, int bound_mode, const uint8_t *codes, void *stream);
+
+/* ---- accumulation (rake and compress) ----------------------------------------
+ * Kernel-level mirrors of pyfastflow/flow/downstream_propag.py with identical
+ * semantics (donor slots in ascending donor index, as the reference's serial
+ * order gives):
+ *   rcv2donor            downstream_propag.py:77-96   (ndnr must be zero on entry)
+ *   rake_compress_accum  downstream_propag.py:99-179  (one round)
+ *   fuse                 downstream_propag.py:59-74 */
+int pff_rcv2donor(const int32_t *rcv, int32_t *dnr, int32_t *ndnr, int N, void *stream);
+int pff_rake_compress_accum(int32_t *dnr, int32_t *ndnr, float *p, int32_t *src, int32_t *dnr_,
+                            int32_t *ndnr_, float *p_, int iteration, int N, void *stream);
+int pff_fuse(float *A, const int32_t *src, const float *B, int iteration, int N, void *stream);
+
+/* Whole accumulation as FlowRouter.accumulate_constant_Q drives it
+ * (pyfastflow/flow/flowfields.py:254-292), for any receiver forest:
+ *   Q      in: per-cell seed (value*dx^2, 1, or per-cell weights); out: upstream sum,
+ *          bit-identical to the reference's f32 rake-and-compress result
+ *   counts out (optional, may be NULL): exact uint32 upstream cell counts
+ * workspace: pff_accumulate_workspace_bytes(N) bytes of device scratch. */
+size_t pff_accumulate_workspace_bytes(int N);
+int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *counts, int N, void *workspace,
+                   size_t workspace_bytes, void *stream);
+
+/* ---- lake / depression rerouting -----------------------------------------------
+ * Replaces pyfastflow/flow/lakeflow.py:466-538 reroute_flow(bid, rec, rec_, rec__,
+ * z, z_prime, is_border, outlet, basin_saddle, basin_saddlenode, tag, tag_,
+ * change, carve).  Same buffers and meaning; rec is rerouted in place (carve) or
+ * the result is left in rec_ (carve = 0, as the reference leaves it).  is_border,
+ * tag, tag_ are uint8 (0/1).  bid ends in the basin_id_init state, as in the
+ * reference.  Synchronizes `stream` (reads pit counts on the host, like the
+ * reference's depression_counter).  n_outer_out (host, optional) receives the
+ * number of outer iterations run.  workspace: pff_reroute_workspace_bytes(N). */
+size_t pff_reroute_workspace_bytes(int N);
+int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                     float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
+                     int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int carve, int nx,
+                     int ny, int bound_mode, const uint8_t *codes, void *workspace,
+                     size_t workspace_bytes, int *n_outer_out, void *stream);
+
+/* Basin labels of a receiver forest: lakeflow.py:82-101 basin_identification
+ * (bid = root+1, or 0 when the root can leave the domain).  rec_ is scratch (N). */
+int pff_basin_identification(int32_t *bid, const int32_t *rec, int32_t *rec_, int nx, int ny,
+                             int bound_mode, const uint8_t *codes, void *stream);
+
+/* lakeflow.py:25-44 depression_counter; writes the count to *count_out (host).
+ * Synchronizes `stream`. */
+int pff_depression_counter(const int32_t *rec, int nx, int ny, int bound_mode,
+                           const uint8_t *codes, int *count_out, void *stream);
+
+/* lakeflow.py:106-281 saddlesort (passes 1-5). */
+int pff_saddlesort(const int32_t *bid, uint8_t *is_border, float *z_prime, int64_t *basin_saddle,
+                   int32_t *basin_saddlenode, int64_t *outlet, const float *z, int nx, int ny,
+                   int bound_mode, const uint8_t *codes, void *stream);
+
+/* ---- GraphFlood ----------------------------------------------------------------
+ * pyfastflow/flow/fill_topo.py:99-125 fill_z_add_delta(zh, h, z_, receivers,
+ * receivers_, receivers__, epsilon): ceil(log2 N) pointer-jumping fill rounds
+ * with increment float(2^(it-1)*epsilon), then h += z_-zh, zh = z_.  The round's
+ * in-place read of z_ (a race in the reference) is pinned to snapshot semantics:
+ * every read of a round sees the start-of-round value.  workspace:
+ * pff_fill_workspace_bytes(N) bytes. */
+size_t pff_fill_workspace_bytes(int N);
+int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_t *receivers,
+                         int32_t *receivers_, int32_t *receivers__, double epsilon, int N,
+                         void *workspace, size_t workspace_bytes, void *stream);
+
+/* graphflood/gf_hydrodynamics.py:24-75 diffuse_Q_constant_prec(zh, Q, temp), run
+ * `nsweeps` times (the Flooder runs 5).  prec_dx2 = float(PREC*DX*DX).  Sums are
+ * formed in the reference's serial order (ascending source cell, then k), so the
+ * result is deterministic.  temp: N floats (ends equal to Q, as in the reference);
+ * workspace: pff_diffuse_workspace_bytes(N). */
+size_t pff_diffuse_workspace_bytes(int N);
+int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps, int nx, int ny, float dx,
+                  float prec_dx2, int bound_mode, const uint8_t *codes, void *workspace,
+                  size_t workspace_bytes, void *stream);
+
+/* graphflood/gf_hydrodynamics.py:79-129 graphflood_core_cte_mannings(h, zh, dh,
+ * rec, Q) with constants dx, dx2 = float(DX**2), manning, edgesw, dt (DT_HYDRO).
+ * If dhmax (device float) and h_ref (device, N) are both non-NULL, dhmax receives
+ * max |h_after - h_ref| (atomically maxed into its current value; zero it first). */
+int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, const float *Q, int N,
+                        float dx, float dx2, float manning, float edgesw, float dt,
+                        const float *h_ref, float *dhmax, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFF_H */

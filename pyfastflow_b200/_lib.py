@@ -1,0 +1,71 @@
+"""Loader for ``libpff.so``, the sm_100a CUDA library behind this package.
+
+The library is built in-tree (``pyfastflow_b200/libpff.so``) by
+``pyfastflow_b200.build.build()``.  There is no fallback: if the library is
+missing every call raises, so a run can never silently compute on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpff.so")
+
+_vp, _i32, _i64, _f32, _f64, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_float, C.c_double, C.c_size_t
+
+# name -> (restype, argtypes); mirrors include/pff.h
+SIGNATURES = {
+    "pff_version": (_i32, []),
+    "pff_last_error_string": (C.c_char_p, []),
+    "pff_launch_count": (C.c_longlong, []),
+    "pff_compute_receivers": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, _vp]),
+    "pff_rcv2donor": (_i32, [_vp, _vp, _vp, _i32, _vp]),
+    "pff_rake_compress_accum": (_i32, [_vp] * 7 + [_i32, _i32, _vp]),
+    "pff_fuse": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
+    "pff_accumulate_workspace_bytes": (_sz, [_i32]),
+    "pff_accumulate": (_i32, [_vp, _vp, _vp, _i32, _vp, _sz, _vp]),
+    "pff_reroute_workspace_bytes": (_sz, [_i32]),
+    "pff_reroute_flow": (_i32, [_vp] * 12 + [_i32, _i32, _i32, _i32, _vp, _vp, _sz, C.POINTER(C.c_int), _vp]),
+    "pff_basin_identification": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),
+    "pff_depression_counter": (_i32, [_vp, _i32, _i32, _i32, _vp, C.POINTER(C.c_int), _vp]),
+    "pff_saddlesort": (_i32, [_vp] * 7 + [_i32, _i32, _i32, _vp, _vp]),
+    "pff_fill_workspace_bytes": (_sz, [_i32]),
+    "pff_fill_z_add_delta": (_i32, [_vp] * 6 + [_f64, _i32, _vp, _sz, _vp]),
+    "pff_diffuse_workspace_bytes": (_sz, [_i32]),
+    "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
+    "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+class PFFError(RuntimeError):
+    pass
+
+
+def load():
+    """Load libpff.so (raises ImportError if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with pyfastflow_b200.build.build() "
+                          "(nvcc, sm_100a); there is no CPU fallback")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args):
+    """Call a libpff entry point and raise PFFError on a nonzero status."""
+    fn = getattr(load(), name)
+    rc = fn(*args)
+    if rc != 0:
+        msg = load().pff_last_error_string().decode(errors="replace")
+        raise PFFError(f"{name} failed with status {rc}: {msg}")
+    return rc

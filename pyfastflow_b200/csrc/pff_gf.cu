@@ -1,0 +1,262 @@
+// libpff GraphFlood: topographic fill with delta, MFD discharge diffusion and
+// the Manning depth update (pyfastflow/flow/fill_topo.py, graphflood/gf_hydrodynamics.py).
+//
+// All f32 arithmetic is written with explicit round-to-nearest intrinsics (and
+// the library is built with -fmad=false), so each operation is the reference's
+// single IEEE operation in the reference's order.
+#include "pff_internal.h"
+
+namespace pff {
+
+// ---- fill (fill_topo.py:17-45, snapshot semantics) ---------------------------
+__global__ void __launch_bounds__(256) k_fill_round(const float *__restrict__ zh, const float *__restrict__ zs,
+                                                    float *__restrict__ zn, const int32_t *__restrict__ ra,
+                                                    int32_t *__restrict__ rb, float inc, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int r = ra[i];
+    const int rr = ra[r];
+    rb[i] = rr;                                            // :29
+    const float zi = zs[i];
+    if (i == r || (zi > zh[r] && rr == r)) { zn[i] = zi; return; }  // :32
+    zn[i] = fmaxf(zi, __fadd_rn(zs[r], inc));              // :36
+}
+
+// _apply_fill_z_add_delta (:82-97)
+__global__ void k_fill_apply(float *zh, float *h, const float *__restrict__ z_, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float zf = z_[i];
+    h[i] = __fadd_rn(h[i], __fsub_rn(zf, zh[i]));
+    zh[i] = zf;
+}
+
+// ---- diffusion (gf_hydrodynamics.py:24-75) -----------------------------------
+// Per-cell outgoing weights fl(tS_k / sums) and a "source" flag (non-outlet
+// with sums != 0), computed once per call: zh does not change between sweeps.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_diffuse_weights(const float *__restrict__ zh, float4 *w, uint8_t *issrc,
+                                                         Grid g, float dx)
+{
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= g.nx || row >= g.ny) return;
+    const int i = row * g.nx + col;
+    if (can_leave<MODE>(g, i, row, col)) { issrc[i] = 0; return; }
+    const float zi = zh[i];
+    float s[4];
+    float sums = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j = neighbour<MODE>(g, i, row, col, k);
+        s[k] = (j != -1) ? fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zh[j]), dx)) : 0.f;
+        sums = __fadd_rn(sums, s[k]);  // j == -1 adds max(0, 0) = 0
+    }
+    if (sums == 0.f) { issrc[i] = 0; return; }
+    issrc[i] = 1;
+    w[i] = make_float4(__fdiv_rn(s[0], sums), __fdiv_rn(s[1], sums), __fdiv_rn(s[2], sums), __fdiv_rn(s[3], sums));
+}
+
+// Candidate donors of j: the grid-adjacent cells and the wrap partners across
+// opposite edges (every neighbour relation of every mode is among these).
+__device__ __forceinline__ int diffuse_candidates(const Grid &g, int j, int row, int col, int *c)
+{
+    int n = 0;
+    const int nx = g.nx, ny = g.ny;
+    if (row > 0) c[n++] = j - nx;
+    if (col > 0) c[n++] = j - 1;
+    if (col < nx - 1) c[n++] = j + 1;
+    if (row < ny - 1) c[n++] = j + nx;
+    if (col == 0) c[n++] = j + nx - 1;
+    if (col == nx - 1) c[n++] = j - nx + 1;
+    if (row == 0) c[n++] = j + nx * (ny - 1);
+    if (row == ny - 1) c[n++] = j - nx * (ny - 1);
+    // ascending, without duplicates
+    for (int a = 1; a < n; ++a) {
+        int x = c[a], b = a - 1;
+        while (b >= 0 && c[b] > x) { c[b + 1] = c[b]; --b; }
+        c[b + 1] = x;
+    }
+    int m = 0;
+    for (int a = 0; a < n; ++a)
+        if (m == 0 || c[m - 1] != c[a]) c[m++] = c[a];
+    return m;
+}
+
+// One sweep in gather form: temp[j] = P*dx^2 + sum over sources i ascending, then
+// k ascending, of fl(w_ik * Q[i]) -- the serial order of the reference's atomics.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__ Q, float *__restrict__ Qn,
+                                                       const float4 *__restrict__ w, const uint8_t *__restrict__ issrc,
+                                                       Grid g, float prec_dx2)
+{
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= g.nx || row >= g.ny) return;
+    const int j = row * g.nx + col;
+    int c[8];
+    const int n = diffuse_candidates(g, j, row, col, c);
+    float acc = prec_dx2;
+    for (int a = 0; a < n; ++a) {
+        const int i = c[a];
+        if (!issrc[i]) continue;
+        const float qi = Q[i];
+        const float4 wi = w[i];
+        const float ww[4] = {wi.x, wi.y, wi.z, wi.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (neighbour_i<MODE>(g, i, k) == j) acc = __fadd_rn(acc, __fmul_rn(ww[k], qi));
+    }
+    Qn[j] = acc;
+}
+
+// ---- Manning update (gf_hydrodynamics.py:79-129) ------------------------------
+// h^(5/3) with the exponent rounded to f32 (Taichi folds 5./3. to an f32
+// constant), evaluated in double and rounded once: the correctly rounded f32
+// power.  Both the oracle and this kernel use this definition.
+__device__ __forceinline__ float pow53(float h) { return (float)pow((double)h, (double)(5.0f / 3.0f)); }
+
+__global__ void __launch_bounds__(256) k_core1(float *h, const float *__restrict__ zh, float *dh,
+                                               const int32_t *__restrict__ rec, const float *__restrict__ Q, int N,
+                                               float dx, float dx2, float manning, float edgesw, float dt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int r = rec[i];
+    float tS = edgesw;
+    if (r != i) tS = fmaxf(__fdiv_rn(__fsub_rn(zh[i], zh[r]), dx), 1e-4f);
+    float Qo = __fmul_rn(dx, pow53(h[i]));
+    Qo = __fdiv_rn(Qo, manning);
+    Qo = __fmul_rn(Qo, __fsqrt_rn(tS));
+    float tdh = __fdiv_rn(__fsub_rn(Q[i], Qo), dx2);
+    tdh = __fmul_rn(tdh, dt);
+    const float h1 = __fadd_rn(h[i], tdh);
+    h[i] = h1;
+    if (h1 < 0.f) tdh = __fadd_rn(tdh, h1);
+    dh[i] = tdh;
+}
+
+__device__ __forceinline__ void atomic_max_abs(float *dst, float v)
+{
+    // |v| >= 0 (or NaN, whose bits exceed +inf): unsigned compare orders them.
+    atomicMax(reinterpret_cast<unsigned int *>(dst), __float_as_uint(fabsf(v)));
+}
+
+__global__ void __launch_bounds__(256) k_core2(float *h, float *zh, const float *__restrict__ dh,
+                                               const float *__restrict__ href, float *dhmax, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float m = 0.f;
+    if (i < N) {
+        const float d = dh[i];
+        const float hn = __fadd_rn(h[i], d);
+        h[i] = hn;
+        zh[i] = __fadd_rn(zh[i], d);
+        if (dhmax && href) m = fabsf(__fsub_rn(hn, href[i]));
+    }
+    if (!dhmax || !href) return;
+    // warp max then one atomic per warp
+    unsigned mu = __float_as_uint(m);
+    for (int o = 16; o; o >>= 1) mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    if ((threadIdx.x & 31) == 0 && mu) atomicMax(reinterpret_cast<unsigned int *>(dhmax), mu);
+}
+
+template <int MODE>
+static void l_diffuse(const float *zh, float *Q, float *temp, float4 *w, uint8_t *issrc, int nsweeps,
+                      const Grid &g, float dx, float prec_dx2, cudaStream_t st)
+{
+    dim3 b(32, 8), gr(div_up(g.nx, 32), div_up(g.ny, 8));
+    { k_diffuse_weights<MODE><<<gr, b, 0, st>>>(zh, w, issrc, g, dx); count_launch(); }
+    float *a = Q, *c = temp;
+    for (int s = 0; s < nsweeps; ++s) {
+        { k_diffuse_sweep<MODE><<<gr, b, 0, st>>>(a, c, w, issrc, g, prec_dx2); count_launch(); }
+        float *t = a; a = c; c = t;
+    }
+}
+
+}  // namespace pff
+
+using namespace pff;
+
+extern "C" size_t pff_fill_workspace_bytes(int N) { return Carver::round(sizeof(float) * (size_t)N) + 256; }
+
+extern "C" int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_t *receivers, int32_t *receivers_,
+                                    int32_t *receivers__, double epsilon, int N, void *workspace,
+                                    size_t workspace_bytes, void *stream)
+{
+    clear_error();
+    if (N <= 1 || !zh || !h || !z_ || !receivers || !receivers_ || !receivers__) {
+        set_error("pff_fill_z_add_delta: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    if (!workspace || workspace_bytes < pff_fill_workspace_bytes(N)) {
+        set_error("pff_fill_z_add_delta: workspace too small");
+        return PFF_ERR_WORKSPACE;
+    }
+    cudaStream_t st = S(stream);
+    Carver cv(workspace, workspace_bytes);
+    float *zt = cv.take<float>(N);
+    const size_t nbf = sizeof(float) * (size_t)N, nbi = sizeof(int32_t) * (size_t)N;
+    PFF_CUDA(cudaMemcpyAsync(z_, zh, nbf, cudaMemcpyDeviceToDevice, st));              // :116
+    PFF_CUDA(cudaMemcpyAsync(receivers_, receivers, nbi, cudaMemcpyDeviceToDevice, st));  // :117
+    int nr = 0;
+    for (long long p = 1; p < N; p <<= 1) ++nr;  // ceil(log2 N), :121
+    float *zs = z_, *zn = zt;
+    int32_t *ra = receivers_, *rb = receivers__;
+    for (int it = 0; it < nr; ++it) {
+        const float inc = (float)(ldexp(1.0, it - 1) * epsilon);  // Python folds 2**(it-1)*eps in double
+        { k_fill_round<<<div_up(N, 256), 256, 0, st>>>(zh, zs, zn, ra, rb, inc, N); count_launch(); }
+        float *tz = zs; zs = zn; zn = tz;
+        int32_t *tr = ra; ra = rb; rb = tr;
+    }
+    if (zs != z_) PFF_CUDA(cudaMemcpyAsync(z_, zs, nbf, cudaMemcpyDeviceToDevice, st));
+    // both receiver buffers end with the final jumped pointers (:39-40)
+    PFF_CUDA(cudaMemcpyAsync(rb, ra, nbi, cudaMemcpyDeviceToDevice, st));
+    { k_fill_apply<<<div_up(N, 256), 256, 0, st>>>(zh, h, z_, N); count_launch(); }
+    return check_cuda("pff_fill_z_add_delta");
+}
+
+extern "C" size_t pff_diffuse_workspace_bytes(int N)
+{
+    return Carver::round(sizeof(float4) * (size_t)N) + Carver::round((size_t)N) + 512;
+}
+
+extern "C" int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps, int nx, int ny, float dx,
+                             float prec_dx2, int bound_mode, const uint8_t *codes, void *workspace,
+                             size_t workspace_bytes, void *stream)
+{
+    clear_error();
+    PFF_TRY(check_grid(nx, ny, bound_mode, codes));
+    if (!zh || !Q || !temp || nsweeps < 0) { set_error("pff_diffuse_q: bad arguments"); return PFF_ERR_ARG; }
+    const int N = nx * ny;
+    if (!workspace || workspace_bytes < pff_diffuse_workspace_bytes(N)) {
+        set_error("pff_diffuse_q: workspace too small");
+        return PFF_ERR_WORKSPACE;
+    }
+    if (nsweeps == 0) return PFF_OK;
+    Grid g{nx, ny, bound_mode, codes};
+    cudaStream_t st = S(stream);
+    Carver cv(workspace, workspace_bytes);
+    float4 *w = cv.take<float4>(N);
+    uint8_t *issrc = cv.take<uint8_t>(N);
+    PFF_MODE_DISPATCH(bound_mode, l_diffuse, zh, Q, temp, w, issrc, nsweeps, g, dx, prec_dx2, st);
+    // the reference ends each sweep with Q == temp (:74-75)
+    const size_t nbf = sizeof(float) * (size_t)N;
+    if (nsweeps & 1) PFF_CUDA(cudaMemcpyAsync(Q, temp, nbf, cudaMemcpyDeviceToDevice, st));
+    else PFF_CUDA(cudaMemcpyAsync(temp, Q, nbf, cudaMemcpyDeviceToDevice, st));
+    return check_cuda("pff_diffuse_q");
+}
+
+extern "C" int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, const float *Q, int N,
+                                   float dx, float dx2, float manning, float edgesw, float dt, const float *h_ref,
+                                   float *dhmax, void *stream)
+{
+    clear_error();
+    if (N <= 0 || !h || !zh || !dh || !rec || !Q) { set_error("pff_graphflood_core: bad arguments"); return PFF_ERR_ARG; }
+    cudaStream_t st = S(stream);
+    { k_core1<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, rec, Q, N, dx, dx2, manning, edgesw, dt); count_launch(); }
+    { k_core2<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, h_ref, dhmax, N); count_launch(); }
+    return check_cuda("pff_graphflood_core");
+}

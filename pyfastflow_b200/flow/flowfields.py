@@ -1,0 +1,159 @@
+"""FlowRouter, mirroring pyfastflow/flow/flowfields.py:26-319.
+
+Holds the same fields as the reference (as torch CUDA tensors, same attribute
+names) and drives the same pipeline: compute_receivers -> reroute_flow ->
+accumulate_constant_Q.  The grid is a runtime argument of every kernel, so
+several routers of different shapes can coexist (the reference allows one grid
+per process).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import constants as cte
+from .. import _dev, _lib
+from . import environment as env
+from .f32_i32_struct import INVALID_KEY
+
+
+class FlowRouter:
+    def __init__(self, nx, ny, dx, boundary_mode="normal", boundaries=None, lakeflow=True,
+                 stochastic_receivers=False, device="cuda"):
+        if stochastic_receivers:
+            raise NotImplementedError("stochastic receivers are not supported")
+        if boundary_mode not in cte.BOUND_MODES:
+            boundary_mode = "normal"  # the reference falls back to mode 0 (flowfields.py:169-175)
+        self.nx, self.ny, self.dx = int(nx), int(ny), float(dx)
+        self.rshp = (self.ny, self.nx)
+        self.boundary_mode = boundary_mode
+        self.mode = cte.BOUND_MODES[boundary_mode]
+        self.lakeflow = lakeflow
+        self.stochastic_receivers = False
+        self.device = torch.device(device)
+        N = self.nx * self.ny
+        self.N = N
+        f32, i32 = dict(dtype=torch.float32, device=self.device), dict(dtype=torch.int32, device=self.device)
+        # core fields (flowfields.py:71-115)
+        self.z = torch.zeros(N, **f32)
+        self.Q = torch.zeros(N, **f32)
+        self.Q_ = torch.zeros(N, **f32)
+        self.gradient = torch.zeros(N, **f32)
+        self.receivers = torch.zeros(N, **i32)
+        self.src = torch.zeros(N, **i32)
+        self.ndonors = torch.zeros(N, **i32)
+        self.ndonors_ = torch.zeros(N, **i32)
+        self.donors = torch.zeros(4 * N, **i32)
+        self.donors_ = torch.zeros(4 * N, **i32)
+        # exact drainage counts (new: the reference accumulates f32 only)
+        self.counts = torch.zeros(N, dtype=torch.int32, device=self.device)
+        self.codes = None
+        if self.mode == 3:
+            if boundaries is None:
+                raise ValueError("custom boundary mode needs a boundaries array")
+            self.codes = torch.from_numpy(np.ascontiguousarray(np.asarray(boundaries, np.uint8).ravel())).to(self.device)
+            if self.codes.numel() != N:
+                raise ValueError("boundaries must have nx*ny entries")
+        self.boundaries = boundaries
+        # lake fields (flowfields.py:119-159); basin arrays sized N+1
+        if lakeflow:
+            self.z_ = torch.zeros(N, **f32)
+            self.z__ = torch.zeros(N, **f32)
+            self.receivers_ = torch.zeros(N, **i32)
+            self.receivers__ = torch.zeros(N, **i32)
+            self.bid = torch.zeros(N, **i32)
+            self.basin_saddlenode = torch.full((N + 1,), -1, **i32)
+            self.outlet = torch.full((N + 1,), INVALID_KEY, dtype=torch.int64, device=self.device)
+            self.basin_saddle = torch.full((N + 1,), INVALID_KEY, dtype=torch.int64, device=self.device)
+            self.is_border = torch.zeros(N, dtype=torch.uint8, device=self.device)
+            self.tag = torch.zeros(N, dtype=torch.uint8, device=self.device)
+            self.tag_ = torch.zeros(N, dtype=torch.uint8, device=self.device)
+            self.change = torch.zeros((), dtype=torch.uint8, device=self.device)
+        self._ws_acc = _dev.Scratch()
+        self._ws_lake = _dev.Scratch()
+        self._ws_fill = _dev.Scratch()
+        self._ws_diff = _dev.Scratch()
+        self.last_n_outer = 0
+        # global configuration, as the reference writes it (flowfields.py:163-182)
+        cte.NX, cte.NY, cte.DX = self.nx, self.ny, self.dx
+        cte.RAND_RCV = False
+        cte.BOUND_MODE = self.mode
+        if self.mode == 3:
+            cte.boundaries = self.codes
+        if not cte.INITIALISED:
+            env.initialise()
+
+    # ---- helpers --------------------------------------------------------------
+    def _codes(self):
+        return self.codes.data_ptr() if self.codes is not None else None
+
+    def free(self):
+        """Release the device fields (flowfields.py:186-200)."""
+        for k in list(vars(self)):
+            if isinstance(getattr(self, k), torch.Tensor):
+                setattr(self, k, None)
+
+    # ---- host I/O ---------------------------------------------------------------
+    def set_z(self, z):
+        """Upload elevations (flowfields.py:202-214); accepts numpy or torch."""
+        if isinstance(z, torch.Tensor):
+            self.z.copy_(z.reshape(-1).to(torch.float32))
+        else:
+            self.z.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(z).ravel().astype(np.float32))))
+
+    def get_Q(self):
+        return self.Q.cpu().numpy().reshape(self.rshp)
+
+    def get_Z(self):
+        return self.z.cpu().numpy().reshape(self.rshp)
+
+    def get_receivers(self):
+        return self.receivers.cpu().numpy().reshape(self.rshp)
+
+    def get_counts(self):
+        """Exact upstream cell counts (uint32) from the last accumulation."""
+        return self.counts.cpu().numpy().view(np.uint32).reshape(self.rshp)
+
+    # ---- pipeline -----------------------------------------------------------------
+    def compute_receivers(self):
+        """flowfields.py:216-226 -> receivers.py:15-58."""
+        _lib.call("pff_compute_receivers", self.z.data_ptr(), self.receivers.data_ptr(), self.gradient.data_ptr(),
+                  self.nx, self.ny, self.dx, self.mode, self._codes(), _dev.stream())
+
+    def reroute_flow(self, carve=True):
+        """flowfields.py:228-252 -> lakeflow.py:466-538."""
+        if not self.lakeflow:
+            raise RuntimeError("Flow field not compiled for lakeflow")
+        import ctypes as C
+
+        n = self.N
+        wp, wn = self._ws_lake.get(_lib.load().pff_reroute_workspace_bytes(n), self.device)
+        nout = C.c_int()
+        _lib.call("pff_reroute_flow", self.bid.data_ptr(), self.receivers.data_ptr(), self.receivers_.data_ptr(),
+                  self.receivers__.data_ptr(), self.z.data_ptr(), self.z_.data_ptr(), self.is_border.data_ptr(),
+                  self.outlet.data_ptr(), self.basin_saddle.data_ptr(), self.basin_saddlenode.data_ptr(),
+                  self.tag.data_ptr(), self.tag_.data_ptr(), int(bool(carve)), self.nx, self.ny, self.mode,
+                  self._codes(), wp, wn, C.byref(nout), _dev.stream())
+        self.last_n_outer = nout.value
+
+    def _accumulate(self, counts: bool = True):
+        wp, wn = self._ws_acc.get(_lib.load().pff_accumulate_workspace_bytes(self.N), self.device)
+        _lib.call("pff_accumulate", self.receivers.data_ptr(), self.Q.data_ptr(),
+                  self.counts.data_ptr() if counts else None, self.N, wp, wn, _dev.stream())
+
+    def accumulate_constant_Q(self, value, area=True, counts=True):
+        """flowfields.py:254-292: Q = value*dx^2 (area) or value per cell,
+        accumulated upstream.  Bit-identical to the reference's f32 result; the
+        exact uint32 upstream cell counts land in ``counts`` as well."""
+        self.Q.fill_(value * (self.dx * self.dx if area else 1.0))
+        self._accumulate(counts)
+
+    def accumulate_weighted_Q(self, weights, counts=True):
+        """Upstream sum of per-cell weights (e.g. precipitation-weighted
+        discharge), the path scripts run by filling Q before rcv2donor
+        (examples/exemple_raw_1.py:135-150)."""
+        if isinstance(weights, torch.Tensor):
+            self.Q.copy_(weights.reshape(-1).to(torch.float32))
+        else:
+            self.Q.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(weights, np.float32).ravel())))
+        self._accumulate(counts)

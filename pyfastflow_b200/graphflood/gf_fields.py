@@ -1,0 +1,81 @@
+"""Flooder, mirroring pyfastflow/graphflood/gf_fields.py:30-159."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import constants as cte
+from .. import _dev, _lib
+from ..flow import fill_topo
+
+
+class Flooder:
+    def __init__(self, router, precipitation_rates=10e-3 / 3600, manning=0.033, edge_slope=1e-2):
+        self.nx, self.ny, self.dx, self.rshp = router.nx, router.ny, router.dx, router.rshp
+        self.router = router
+        N = router.N
+        self.h = torch.zeros(N, dtype=torch.float32, device=router.device)
+        self.dh = torch.zeros(N, dtype=torch.float32, device=router.device)
+        self._h0 = torch.zeros(N, dtype=torch.float32, device=router.device)
+        self._dhmax = torch.zeros(1, dtype=torch.float32, device=router.device)
+        self.precipitation_rates = precipitation_rates
+        self.manning = manning
+        self.edge_slope = edge_slope
+        cte.PREC = precipitation_rates  # gf_fields.py:106-108
+        cte.MANNING = manning
+        cte.EDGESW = edge_slope
+
+    def _consts(self):
+        f = lambda x: float(np.float32(x))  # noqa: E731  (Python folds in double, the kernel sees f32)
+        return dict(dx=f(self.dx), dx2=f(self.dx ** 2), prec_dx2=f(self.precipitation_rates * self.dx * self.dx),
+                    manning=f(self.manning), edgesw=f(self.edge_slope), dt=f(cte.DT_HYDRO))
+
+    def iteration(self, track_dh: bool = False):
+        """One GraphFlood iteration (gf_fields.py:126-141): receivers, carve
+        reroute, fill with delta (epsilon 1e-3), 5 diffusion sweeps, Manning update."""
+        r = self.router
+        c = self._consts()
+        st = _dev.stream()
+        if track_dh:
+            self._h0.copy_(self.h)
+            self._dhmax.zero_()
+        r.compute_receivers()
+        r.reroute_flow()
+        fill_topo.fill_z_add_delta(r.z, self.h, r.z_, r.receivers, r.receivers_, r.receivers__, epsilon=1e-3,
+                                   workspace=r._ws_fill)
+        wp, wn = r._ws_diff.get(_lib.load().pff_diffuse_workspace_bytes(r.N), r.device)
+        _lib.call("pff_diffuse_q", r.z.data_ptr(), r.Q.data_ptr(), r.Q_.data_ptr(), 5, r.nx, r.ny, c["dx"],
+                  c["prec_dx2"], r.mode, r._codes(), wp, wn, st)
+        _lib.call("pff_graphflood_core", self.h.data_ptr(), r.z.data_ptr(), self.dh.data_ptr(),
+                  r.receivers.data_ptr(), r.Q.data_ptr(), r.N, c["dx"], c["dx2"], c["manning"], c["edgesw"],
+                  c["dt"], self._h0.data_ptr() if track_dh else None, self._dhmax.data_ptr() if track_dh else None,
+                  st)
+
+    def run_graphflood(self, N=10):
+        """N iterations (gf_fields.py:111-141)."""
+        for _ in range(N):
+            self.iteration()
+
+    def run_to_residual(self, tol_ratio=1e-4, max_iter=20000, check_every=1):
+        """Iterate until max|dh|/dt < tol_ratio * precipitation rate or max_iter.
+        Returns (iterations, stop_reason, residual) with stop_reason in
+        {"residual", "max_iter"}; dh is the change of h over one iteration."""
+        thr = tol_ratio * self.precipitation_rates
+        res = float("inf")
+        for it in range(1, max_iter + 1):
+            track = (it % check_every) == 0
+            self.iteration(track_dh=track)
+            if track:
+                res = float(self._dhmax.item()) / cte.DT_HYDRO
+                if res < thr:
+                    return it, "residual", res
+        return max_iter, "max_iter", res
+
+    def set_h(self, val):
+        if isinstance(val, torch.Tensor):
+            self.h.copy_(val.reshape(-1).to(torch.float32))
+        else:
+            self.h.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(val, np.float32).ravel())))
+
+    def get_h(self):
+        return self.h.cpu().numpy().reshape(self.rshp)

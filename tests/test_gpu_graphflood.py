@@ -1,0 +1,112 @@
+"""GraphFlood kernels vs the oracle: fill (snapshot rounds), diffusion (serial
+summation order), Manning update, and whole Flooder iterations -- bit-exact."""
+import numpy as np
+import pytest
+
+from pyfastflow_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def bits(a):
+    return np.asarray(a, np.float32).view(np.uint32)
+
+
+def state(orc, nx, ny, mode, seed, h_scale=0.5):
+    rng = np.random.default_rng(seed)
+    z = synthetic.spectral_dem(nx, ny, seed, relief=50.0, npits=20, pit_scale=0.2)
+    h = (rng.random(nx * ny) * h_scale).astype(np.float32)
+    zh = (z.ravel() + h).astype(np.float32)
+    og = orc.Grid(nx, ny, mode)
+    rcv, _ = orc.compute_receivers(zh, og, 10.0)
+    rcv, _, _, _, _ = orc.reroute_flow(rcv, zh, og)
+    return og, zh, h, rcv
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_fill_z_add_delta(orc, cuda, mode):
+    torch = cuda
+    from pyfastflow_b200 import flow
+
+    og, zh, h, rcv = state(orc, 150, 110, mode, 3)
+    zd, hd = dev(torch, zh), dev(torch, h)
+    z_ = torch.zeros_like(zd)
+    r_, r__ = torch.zeros(og.N, dtype=torch.int32, device="cuda"), torch.zeros(og.N, dtype=torch.int32, device="cuda")
+    flow.fill_z_add_delta(zd, hd, z_, dev(torch, rcv), r_, r__, epsilon=1e-3)
+    zo, ho, z_o = orc.fill_z_add_delta(zh.copy(), h.copy(), rcv, eps=1e-3)
+    assert np.array_equal(bits(host(zd)), bits(zo))
+    assert np.array_equal(bits(host(hd)), bits(ho))
+    assert np.array_equal(bits(host(z_)), bits(z_o))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_diffuse(orc, cuda, mode):
+    torch = cuda
+    from pyfastflow_b200 import constants as cte
+    from pyfastflow_b200.graphflood import diffuse_Q_constant_prec
+
+    nx, ny = 131, 97
+    rng = np.random.default_rng(mode)
+    zh = synthetic.spectral_dem(nx, ny, 5, relief=20.0).ravel()
+    codes = None
+    if mode == 3:
+        codes = rng.choice(np.array([1, 1, 1, 1, 3, 0, 9], np.uint8), nx * ny)
+    og = orc.Grid(nx, ny, mode, codes)
+    Q = (rng.random(nx * ny) * 10).astype(np.float32)
+    cte.NX, cte.NY, cte.DX, cte.BOUND_MODE, cte.PREC = nx, ny, 10.0, mode, 1e-5
+    cte.boundaries = dev(torch, codes) if codes is not None else None
+    Qd, tmp = dev(torch, Q), torch.zeros(nx * ny, dtype=torch.float32, device="cuda")
+    diffuse_Q_constant_prec(dev(torch, zh), Qd, tmp, nsweeps=5)
+    Qo = Q.copy()
+    for _ in range(5):
+        orc.diffuse_q(zh, Qo, og, 10.0, 1e-5)
+    assert np.array_equal(bits(host(Qd)), bits(Qo))
+    assert np.array_equal(bits(host(tmp)), bits(Qo))
+
+
+def test_manning_core(orc, cuda):
+    torch = cuda
+    from pyfastflow_b200 import constants as cte
+    from pyfastflow_b200.graphflood import graphflood_core_cte_mannings
+
+    og, zh, h, rcv = state(orc, 128, 128, 0, 9, h_scale=0.2)
+    rng = np.random.default_rng(1)
+    Q = (rng.random(og.N) * 50).astype(np.float32)
+    h[::17] = -0.01  # negative depths take the reference's NaN path
+    cte.DX, cte.MANNING, cte.EDGESW, cte.DT_HYDRO = 10.0, 0.033, 1e-2, 5e-3
+    hd, zd, dh = dev(torch, h), dev(torch, zh), torch.zeros(og.N, dtype=torch.float32, device="cuda")
+    graphflood_core_cte_mannings(hd, zd, dh, dev(torch, rcv), dev(torch, Q))
+    ho, zo, dho = orc.graphflood_core(h.copy(), zh.copy(), rcv, Q, 10.0, 0.033, 1e-2, 5e-3)
+    assert np.array_equal(bits(host(hd)), bits(ho))
+    assert np.array_equal(bits(host(zd)), bits(zo))
+    assert np.array_equal(bits(host(dh)), bits(dho))
+    assert np.isnan(host(hd)[::17]).all()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_flooder_iterations(orc, cuda, mode):
+    """Flooder.run_graphflood vs the oracle's run of the same iterations."""
+    import pyfastflow_b200 as pf
+
+    nx, ny, dx, P = 160, 128, 10.0, 1e-5
+    z = synthetic.spectral_dem(nx, ny, 13, relief=60.0, npits=10, pit_scale=0.2)
+    router = pf.flow.FlowRouter(nx, ny, dx, boundary_mode=["normal", "periodic_EW"][mode])
+    router.set_z(z)
+    fl = pf.graphflood.Flooder(router, precipitation_rates=P, manning=0.033, edge_slope=1e-2)
+    fl.run_graphflood(6)
+    og = orc.Grid(nx, ny, mode)
+    zh = z.ravel().copy()
+    h = np.zeros(nx * ny, np.float32)
+    Q = np.zeros(nx * ny, np.float32)
+    orc.graphflood_run(zh, h, Q, og, dx, P, niter=6)
+    assert np.array_equal(bits(fl.get_h().ravel()), bits(h))
+    assert np.array_equal(bits(router.get_Z().ravel()), bits(zh))
+    assert np.array_equal(bits(router.get_Q().ravel()), bits(Q))

@@ -45,6 +45,10 @@ const char *pff_last_error_string(void);
 /* Total number of CUDA kernels this library has launched in this process (no
  * counterpart in the reference: used to report GPU launches per step). */
 long long pff_launch_count(void);
+/* Make `device` current for this library's calls on the calling host thread
+ * (the library links its own CUDA runtime; callers that use several GPUs set
+ * the device that owns the buffers before calling).  No reference counterpart. */
+int pff_set_device(int device);
 
 /* ---- receivers --------------------------------------------------------------
  * Replaces pyfastflow/flow/receivers.py:15-58 compute_receivers(z, receivers,

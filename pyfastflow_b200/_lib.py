@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpff.so")
@@ -19,6 +20,7 @@ SIGNATURES = {
     "pff_version": (_i32, []),
     "pff_last_error_string": (C.c_char_p, []),
     "pff_launch_count": (C.c_longlong, []),
+    "pff_set_device": (_i32, [_i32]),
     "pff_compute_receivers": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, _vp]),
     "pff_rcv2donor": (_i32, [_vp, _vp, _vp, _i32, _vp]),
     "pff_rake_compress_accum": (_i32, [_vp] * 7 + [_i32, _i32, _vp]),
@@ -61,8 +63,26 @@ def load():
     return lib
 
 
+_tls = threading.local()
+
+
+def _sync_device():
+    """Keep the library's current device equal to torch's (per host thread)."""
+    import torch
+
+    if not torch.cuda.is_available():
+        return  # host-side argument checks still run and report through the status
+    d = torch.cuda.current_device()
+    if getattr(_tls, "device", None) != d:
+        rc = load().pff_set_device(d)
+        if rc != 0:
+            raise PFFError(f"pff_set_device({d}) failed: {load().pff_last_error_string().decode()}")
+        _tls.device = d
+
+
 def call(name: str, *args):
     """Call a libpff entry point and raise PFFError on a nonzero status."""
+    _sync_device()
     fn = getattr(load(), name)
     rc = fn(*args)
     if rc != 0:

@@ -91,6 +91,13 @@ extern "C" int pff_version(void) { return 100; }
 extern "C" const char *pff_last_error_string(void) { return g_err; }
 extern "C" long long pff_launch_count(void) { return g_launches.load(); }
 
+extern "C" int pff_set_device(int device)
+{
+    clear_error();
+    PFF_CUDA(cudaSetDevice(device));
+    return PFF_OK;
+}
+
 extern "C" int pff_compute_receivers(const float *z, int32_t *receivers, float *gradient, int nx,
                                      int ny, float dx, int bound_mode, const uint8_t *codes,
                                      void *stream)

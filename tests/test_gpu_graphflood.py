@@ -17,7 +17,12 @@ def host(t):
 
 
 def bits(a):
-    return np.asarray(a, np.float32).view(np.uint32)
+    """Bit patterns, with every NaN mapped to one value: NaN positions must match,
+    NaN payloads (0x7fffffff on the GPU, 0xffc00000 on x86) need not."""
+    a = np.asarray(a, np.float32)
+    b = a.view(np.uint32).copy()
+    b[np.isnan(a)] = 0x7FC00000
+    return b
 
 
 def state(orc, nx, ny, mode, seed, h_scale=0.5):

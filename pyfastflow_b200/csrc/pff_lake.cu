@@ -9,7 +9,9 @@
 //   - saddlesort pass 5: the serial in-place result, computed as snapshot
 //     decisions plus the one basin whose serial outcome can differ
 //     (k_saddle_p5_serial_fix).
+#include <cub/block/block_scan.cuh>
 #include "pff_internal.h"
+#include "pff_tiles.cuh"
 
 namespace pff {
 
@@ -271,6 +273,362 @@ __global__ void k_carve_link_outlets(int32_t *rec, const int32_t *__restrict__ s
     else rec[snode[b]] = key_index(o);
 }
 
+
+// ---- tile-resolved labels (D4 receivers) ---------------------------------------
+//
+// Pass T: one CTA per 64x32 tile.  Receivers are loaded into shared memory as
+// tile-local pointers; pointer jumping in shared memory brings every cell to its
+// tile terminal -- a root inside the tile, or the last in-tile cell of its path.
+// J[i] = the root, or the receiver of the exit cell (a border cell of the next
+// tile).  Border cells also seed R[i] = J[i].  The same pass lists the pits
+// (interior self-receivers) and the border cells.
+// Pass B: pointer jumping on R over border cells only (a few rounds).
+// Pass L: bid[i] = label of root(i) = Rget(J[i]).
+
+__device__ __forceinline__ int r_get(const int32_t *R, int nx, int ny, int x)
+{
+    return is_tile_border_i(nx, ny, x) ? R[x] : x;
+}
+
+template <int BS>
+__device__ __forceinline__ void block_append(bool pred, int val, int *list, int *count)
+{
+    using Scan = cub::BlockScan<int, BS>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int base;
+    int ex, tot;
+    Scan(tmp).ExclusiveSum(pred ? 1 : 0, ex, tot);
+    if (threadIdx.x == 0) base = tot ? atomicAdd(count, tot) : 0;
+    __syncthreads();
+    if (pred) list[base + ex] = val;
+    __syncthreads();
+}
+
+// info[0] pits, info[1] border cells, info[2] set if some exit target is not a
+// tile-border cell (receivers that are not D4 neighbours)
+template <int MODE>
+__global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *__restrict__ rec, int32_t *J, int32_t *R,
+                                                                int *pits, int *borders, int *info, Grid g)
+{
+    __shared__ int p[TILE_CELLS];
+    __shared__ int ext[TILE_CELLS];
+    const int nx = g.nx, ny = g.ny;
+    const int tx = blockIdx.x, ty = blockIdx.y;
+    const int col0 = tx * TILE_W, row0 = ty * TILE_H;
+    const int w = min(TILE_W, nx - col0), h = min(TILE_H, ny - row0);
+    int gi[TILE_PER_THREAD];
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; ++k) {
+        const int c = threadIdx.x + k * TILE_THREADS;
+        const int lx = c % TILE_W, ly = c / TILE_W;
+        const bool valid = lx < w && ly < h;
+        const int i = valid ? (row0 + ly) * nx + col0 + lx : -1;
+        gi[k] = i;
+        int pc = c, e = -2;
+        if (valid) {
+            const int r = rec[i];
+            if (r == i) {
+                e = -1;
+            } else {
+                const int rr = r / nx, rc = r - rr * nx;
+                if (rr >= row0 && rr < row0 + h && rc >= col0 && rc < col0 + w) {
+                    pc = (rr - row0) * TILE_W + (rc - col0);
+                } else {
+                    e = r;
+                }
+            }
+        }
+        p[c] = pc;
+        ext[c] = e;
+    }
+    __syncthreads();
+    // at most ceil(log2 2048) = 11 rounds for any acyclic in-tile path
+    for (int round = 0; round < 12; ++round) {
+        bool ch = false;
+#pragma unroll
+        for (int k = 0; k < TILE_PER_THREAD; ++k) {
+            const int c = threadIdx.x + k * TILE_THREADS;
+            const int q = p[c];
+            const int qq = p[q];
+            if (qq != q) { p[c] = qq; ch = true; }
+        }
+        if (!__syncthreads_or(ch)) break;
+    }
+#pragma unroll
+    for (int k = 0; k < TILE_PER_THREAD; ++k) {
+        const int c = threadIdx.x + k * TILE_THREADS;
+        const int i = gi[k];
+        bool pit = false, border = false;
+        if (i >= 0) {
+            const int t = p[c];
+            const int e = ext[t];
+            const int j = (e == -1) ? (row0 + t / TILE_W) * nx + col0 + (t % TILE_W) : e;
+            J[i] = j;
+            const int lx = c % TILE_W, ly = c / TILE_W;
+            border = lx == 0 || ly == 0 || lx == w - 1 || ly == h - 1;
+            if (border) R[i] = j;
+            if (e >= 0 && !is_tile_border_i(nx, ny, e)) info[2] = 1;  // receivers are not D4
+            pit = ext[c] == -1 && !can_leave<MODE>(g, i, row0 + ly, col0 + lx);
+        }
+        block_append<TILE_THREADS>(pit, i, pits, info + 0);
+        block_append<TILE_THREADS>(border, i, borders, info + 1);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_border_jump(int32_t *R, const int *__restrict__ borders, const int *nb,
+                                                     int nx, int ny, int r, int *flags)
+{
+    if (r > 0 && *(volatile int *)(flags + r - 1) == 0) return;
+    const int n = *nb;
+    bool ch = false;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int e = borders[k];
+        const int x = R[e];
+        const int y = r_get(R, nx, ny, x);
+        if (y != x) { R[e] = y; ch = true; }
+    }
+    if (__syncthreads_or(ch) && threadIdx.x == 0) flags[r] = 1;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_labels_final(const int32_t *__restrict__ J, const int32_t *__restrict__ R,
+                                                      int32_t *bid, Grid g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.N()) return;
+    const int root = r_get(R, g.nx, g.ny, J[i]);
+    bid[i] = can_leave_i<MODE>(g, root) ? 0 : root + 1;
+}
+
+// ---- list-driven saddle passes ---------------------------------------------------
+
+// reset the basin entries of a pit list (basin = pit + 1) and entry 0
+__global__ void k_basin_reset_list(long long *saddle, long long *outlet, int32_t *snode, uint8_t *inv,
+                                   const int *__restrict__ pits, const int *np)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= n; k += gridDim.x * blockDim.x) {
+        const int b = k < n ? pits[k] + 1 : 0;
+        saddle[b] = iv;
+        outlet[b] = iv;
+        snode[b] = -1;
+        inv[b] = 0;
+    }
+}
+
+// pass 1+2 as k_saddle_p12, also listing the border cells for pass 3
+template <int MODE>
+__global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restrict__ bid, uint8_t *is_border,
+                                                         float *zp, long long *saddle, const float *__restrict__ z,
+                                                         Grid g, int *blist, int *nblist)
+{
+    const int col = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int row = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const bool in = col < g.nx && row < g.ny;
+    const int i = row * g.nx + col;
+    bool border = false;
+    if (in) {
+        const float zi = z[i];
+        if (can_leave<MODE>(g, i, row, col)) {
+            zp[i] = zi;
+        } else {
+            const int bi = bid[i];
+            int js[4];
+            float zn = 1e9f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int j = neighbour<MODE>(g, i, row, col, k);
+                js[k] = j;
+                if (j != -1 && bid[j] != bi) { border = true; zn = fminf(zn, z[j]); }
+            }
+            is_border[i] = border;
+            const float zpi = border ? fmaxf(zi, zn) : 1e9f;
+            zp[i] = zpi;
+            if (border) {
+                const long long iv = invalid_key();
+                long long res = iv;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int j = js[k];
+                    if (j == -1) continue;
+                    const int bj = bid[j];
+                    if (bj != bi) {
+                        const long long c = pack_key(zpi, bj);
+                        res = c < res ? c : res;
+                    }
+                }
+                if (res != iv) atomicMin(saddle + bi, res);
+            }
+        }
+    }
+    block_append<256>(border && bid[i] != 0, i, blist, nblist);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_saddle_p3_list(const int32_t *__restrict__ bid, const float *__restrict__ zp,
+                                                        const long long *__restrict__ saddle, int32_t *snode, Grid g,
+                                                        const int *__restrict__ blist, const int *nblist)
+{
+    const int n = *nblist;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = blist[k];
+        const int bi = bid[i];
+        const long long s = saddle[bi];
+        const float tz = key_value(s);
+        const int tb = key_index(s);
+        const float zpi = zp[i];
+        bool here = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = neighbour_i<MODE>(g, i, q);
+            if (j != -1 && bid[j] == tb && zpi == tz) here = true;
+        }
+        if (here) atomicMax(snode + bi, i);
+    }
+}
+
+template <int MODE>
+__global__ void k_saddle_p4_list(const int32_t *__restrict__ bid, const long long *__restrict__ saddle,
+                                 const int32_t *__restrict__ snode, long long *outlet, const float *__restrict__ z,
+                                 Grid g, const int *__restrict__ pits, const int *np)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = pits[k] + 1;
+        if (b >= g.N() || saddle[b] == iv) continue;  // the reference's pass 4 loop stops at N-1
+        const int node = snode[b];
+        if (node < 0) continue;
+        float tz = 1e9f;
+        int r = -1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = neighbour_i<MODE>(g, node, q);
+            if (j == -1) continue;
+            const float zj = z[j];
+            if (bid[j] != b && tz > zj) { tz = zj; r = j; }
+        }
+        if (r > -1) {
+            const long long c = pack_key(tz, r);
+            if (c < outlet[b]) outlet[b] = c;
+        }
+    }
+}
+
+__global__ void k_saddle_p5_decide_list(const int32_t *__restrict__ bid, const long long *__restrict__ outlet,
+                                        uint8_t *inv, int N, const int *__restrict__ pits, const int *np)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = pits[k] + 1;
+        if (b >= N) continue;
+        const long long o = outlet[b];
+        if (o == iv) continue;
+        const int bd1 = bid[key_index(o)];
+        if (bd1 == 0) continue;
+        const int ro2 = key_index(outlet[bd1]);
+        const int bd2 = (ro2 >= 0 && ro2 < N) ? bid[ro2] : -1;
+        if (bd2 == b && bd1 < b) inv[b] = 1;
+    }
+}
+
+__global__ void k_saddle_p5_apply_list(long long *saddle, long long *outlet, int32_t *snode,
+                                       const uint8_t *__restrict__ inv, int N, const int *__restrict__ pits,
+                                       const int *np)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = pits[k] + 1;
+        if (b >= N || !inv[b]) continue;
+        outlet[b] = iv;
+        saddle[b] = iv;
+        snode[b] = -1;
+    }
+}
+
+// ---- carving by tile-granular path walks ------------------------------------------
+//
+// W1: for every basin with a saddle node, walk its path to the pit one tile at a
+//     time through J (tile terminal pointers) and list the segment starts.
+// W2: walk each segment inside its tile: tag the cells and reverse the links
+//     (rec[next] = cell, lakeflow.py:395-397); the old receivers are read from
+//     rec_, which stays unchanged until every walk is done.
+// Link: rec[saddle node] = outlet node (:399-403).  Every write to rec is also
+// recorded, then replayed onto rec_ so both end equal, as in the reference.
+__global__ void k_carve_segments(const int32_t *__restrict__ snode, const int32_t *__restrict__ rec0,
+                                 const int32_t *__restrict__ J, const int *__restrict__ pits, const int *np, int N,
+                                 int *segs, int *nsegs, int cap, int *err)
+{
+    const int n = *np;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = pits[k] + 1;
+        if (b >= N) continue;
+        int x = snode[b];
+        if (x < 0) continue;
+        for (int step = 0; step < N; ++step) {
+            const int slot = atomicAdd(nsegs, 1);
+            if (slot < cap) segs[slot] = x;
+            else { *err = 1; break; }
+            if (rec0[x] == x) break;
+            x = J[x];
+        }
+    }
+}
+
+__global__ void k_carve_walk(const int32_t *__restrict__ rec0, int32_t *rec, uint8_t *tag, uint8_t *tag_,
+                             const int *__restrict__ segs, const int *nsegs, int cap, int nx, int *mods, int *nmods,
+                             int mcap, int *err)
+{
+    const int n = min(*nsegs, cap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int start = segs[k];
+        int x = start;
+        for (int step = 0; step < TILE_CELLS + 1; ++step) {
+            tag[x] = 1;
+            tag_[x] = 1;
+            const int nxt = rec0[x];
+            if (nxt == x) break;
+            rec[nxt] = x;
+            const int slot = atomicAdd(nmods, 1);
+            if (slot < mcap) { mods[2 * slot] = nxt; mods[2 * slot + 1] = x; }
+            else *err = 1;
+            if (!same_tile(nx, nxt, start)) break;
+            x = nxt;
+        }
+    }
+}
+
+__global__ void k_carve_link_list(int32_t *rec, const int32_t *__restrict__ snode, const long long *__restrict__ outlet,
+                                  const int *__restrict__ pits, const int *np, int N, int *mods, int *nmods, int mcap,
+                                  int *err)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int b = pits[k] + 1;
+        if (b >= N) continue;
+        const long long o = outlet[b];
+        if (o == iv) continue;
+        const int s = snode[b], v = key_index(o);
+        rec[s] = v;
+        const int slot = atomicAdd(nmods, 1);
+        if (slot < mcap) { mods[2 * slot] = s; mods[2 * slot + 1] = v; }
+        else *err = 1;
+    }
+}
+
+// replay onto rec_; order does not matter: every position is written once
+__global__ void k_apply_mods(int32_t *dst, const int *__restrict__ mods, const int *nmods, int mcap)
+{
+    const int n = min(*nmods, mcap);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        dst[mods[2 * k]] = mods[2 * k + 1];
+    }
+}
+
 // ---- launchers ---------------------------------------------------------------
 
 template <int MODE>
@@ -296,6 +654,33 @@ static void l_saddle(const int32_t *bid, uint8_t *isb, float *zp, long long *sad
     { k_saddle_p5_decide<<<div_up(N, 256), 256, 0, st>>>(bid, outlet, inv, N); count_launch(); }
     { k_saddle_p5_serial_fix<<<1, 32, 0, st>>>(bid, outlet, inv, N); count_launch(); }
     { k_saddle_p5_apply<<<div_up(N, 256), 256, 0, st>>>(saddle, outlet, snode, inv, N); count_launch(); }
+}
+
+template <int MODE>
+static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pits, int *borders, int *info,
+                            const Grid &g, cudaStream_t st)
+{
+    dim3 gr(div_up(g.nx, TILE_W), div_up(g.ny, TILE_H));
+    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, borders, info, g); count_launch(); }
+}
+template <int MODE>
+static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, cudaStream_t st)
+{
+    { k_labels_final<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(J, R, bid, g); count_launch(); }
+}
+template <int MODE>
+static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long long *saddle, int32_t *snode,
+                           long long *outlet, uint8_t *inv, const float *z, const Grid &g, const int *pits,
+                           const int *np, int *blist, int *nblist, int grid, cudaStream_t st)
+{
+    const int N = g.N();
+    dim3 gr(div_up(g.nx, 32), div_up(g.ny, 8));
+    { k_saddle_p12_list<MODE><<<gr, 256, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist); count_launch(); }
+    { k_saddle_p3_list<MODE><<<grid, 256, 0, st>>>(bid, zp, saddle, snode, g, blist, nblist); count_launch(); }
+    { k_saddle_p4_list<MODE><<<grid, 256, 0, st>>>(bid, saddle, snode, outlet, z, g, pits, np); count_launch(); }
+    { k_saddle_p5_decide_list<<<grid, 256, 0, st>>>(bid, outlet, inv, N, pits, np); count_launch(); }
+    { k_saddle_p5_serial_fix<<<1, 32, 0, st>>>(bid, outlet, inv, N); count_launch(); }
+    { k_saddle_p5_apply_list<<<grid, 256, 0, st>>>(saddle, outlet, snode, inv, N, pits, np); count_launch(); }
 }
 
 int launch_basin_init(int32_t *bid, const Grid &g, cudaStream_t st)
@@ -388,8 +773,71 @@ extern "C" int pff_saddlesort(const int32_t *bid, uint8_t *is_border, float *z_p
 
 extern "C" size_t pff_reroute_workspace_bytes(int N)
 {
-    return Carver::round((size_t)N + 1) + Carver::round(sizeof(int) * (size_t)N) + Carver::round(sizeof(int) * 256) + 4096;
+    const size_t n = (size_t)N;
+    return Carver::round(n + 1) + Carver::round(4 * n) * 6 + Carver::round(8 * n) + Carver::round(sizeof(int) * 512) +
+           4096;
 }
+
+namespace pff {
+
+struct RerouteWs {
+    uint8_t *inv;
+    int32_t *R;
+    int *pits[2];
+    int *borders, *blist, *segs, *mods;
+    int *ctr;  // [16*p + 0] pits, +1 borders, +2 non-D4 flag (parity p); [40] nblist, [41] nsegs, [42] nmods,
+               // [43] error; [64..127] border-jump round flags; [128..191] label round flags
+};
+
+static RerouteWs carve_ws(void *workspace, size_t bytes, int N)
+{
+    Carver cv(workspace, bytes);
+    RerouteWs w;
+    w.inv = cv.take<uint8_t>((size_t)N + 1);
+    w.R = cv.take<int32_t>(N);
+    w.pits[0] = cv.take<int>(N);
+    w.pits[1] = cv.take<int>(N);
+    w.borders = cv.take<int>(N);
+    w.blist = cv.take<int>(N);
+    w.segs = cv.take<int>(N);
+    w.mods = cv.take<int>(2 * (size_t)N);
+    w.ctr = cv.take<int>(512);
+    return w;
+}
+
+// Tile pass over the receivers `rec`: tile terminals J into Jbuf, pit list and
+// count (read back), border list.  *nonlocal_host is set if some receiver is not
+// a D4 neighbour (then the tile labels do not apply).
+static int tile_pass(const int32_t *rec, int32_t *Jbuf, const Grid &g, RerouteWs &w, int parity, int *npits_host,
+                     int *nonlocal_host, cudaStream_t st)
+{
+    int *info = w.ctr + 16 * parity;
+    PFF_CUDA(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
+    PFF_MODE_DISPATCH(g.mode, l_tile_terminal, rec, Jbuf, w.R, w.pits[parity], w.borders, info, g, st);
+    int h[4];
+    PFF_CUDA(cudaMemcpyAsync(h, info, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PFF_CUDA(cudaStreamSynchronize(st));
+    *npits_host = h[0];
+    *nonlocal_host = h[2];
+    return check_cuda("tile_pass");
+}
+
+// Basin labels from a tile pass: pointer jumping over border cells, then one
+// gather per cell.
+static int tile_resolve(const int32_t *Jbuf, int32_t *bid, const Grid &g, RerouteWs &w, int parity, int grid,
+                        cudaStream_t st)
+{
+    int *info = w.ctr + 16 * parity;
+    int *flags = w.ctr + 64;
+    PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
+    for (int r = 0; r < 32; ++r) {
+        { k_border_jump<<<grid, 256, 0, st>>>(w.R, w.borders, info + 1, g.nx, g.ny, r, flags); count_launch(); }
+    }
+    PFF_MODE_DISPATCH(g.mode, l_labels_final, Jbuf, w.R, bid, g, st);
+    return check_cuda("tile_resolve");
+}
+
+}  // namespace pff
 
 extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
                                 float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
@@ -411,54 +859,102 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
     }
     Grid g{nx, ny, bound_mode, codes};
     cudaStream_t st = S(stream);
-    Carver cv(workspace, workspace_bytes);
-    uint8_t *inv = cv.take<uint8_t>((size_t)N + 1);
-    int *pits = cv.take<int>(N);
-    int *ctr = cv.take<int>(256);  // [0] pit count, [64..127] label flags, [128..191] carve flags
-    int *lflags = ctr + 64, *cflags = ctr + 128;
+    RerouteWs w = carve_ws(workspace, workspace_bytes, N);
     long long *sad = (long long *)basin_saddle, *out = (long long *)outlet;
     const size_t nb4 = sizeof(int32_t) * (size_t)N;
     const int B = 256, nbk = div_up(N, B);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = nsm * 8;
     if (n_outer_out) *n_outer_out = 0;
 
     PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :491
-    int Ndep = 0;
-    PFF_TRY(count_pits(rec, g, ctr, nullptr, &Ndep, st));  // :493
-    if (Ndep == 0) return PFF_OK;
-    const int outer = ceil_log2(Ndep) + 1;  // :500
-    const int carve_rounds = ceil_log2(N) + 2;
-    int n_outer = 0;
-    for (int it = 0; it < outer; ++it) {
-        int nd_bis = 0;
-        PFF_TRY(count_pits(rec_, g, ctr, nullptr, &nd_bis, st));  // :501
-        PFF_TRY(launch_basin_init(bid, g, st));                   // :507
-        PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-        PFF_TRY(run_labels(bid, rec__, g, lflags, st));  // :510-511
-        ++n_outer;
-        if (nd_bis == 0) break;  // :512
-        PFF_MODE_DISPATCH(bound_mode, l_saddle, bid, is_border, z_prime, sad, basin_saddlenode, out, inv, z, g, st);
+    PFF_CUDA(cudaMemsetAsync(w.ctr, 0, 512 * sizeof(int), st));
+    int outer = 0, n_outer = 0;
+    for (int it = 0;; ++it) {
+        if (it > 0 && it >= outer) break;  // :500
+        const int par = it & 1;
+        int *np = w.ctr + 16 * par;
+        int nd_bis = 0, nonlocal = 1;
+        // depression_counter(rec_) (:493, :501), with the pit list
         if (carve) {
-            // reroute_carve :424-438
-            PFF_CUDA(cudaMemsetAsync(tag, 0, (size_t)N, st));
-            { k_carve_tag_saddles<<<nbk, B, 0, st>>>(basin_saddlenode, tag, N); count_launch(); }
-            PFF_CUDA(cudaMemcpyAsync(tag_, tag, (size_t)N, cudaMemcpyDeviceToDevice, st));
-            PFF_CUDA(cudaMemcpyAsync(rec, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+            PFF_TRY(tile_pass(rec_, rec__, g, w, par, &nd_bis, &nonlocal, st));
+        } else {
+            PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
+            PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);
+            PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PFF_CUDA(cudaStreamSynchronize(st));
+        }
+        if (it == 0) {
+            if (nd_bis == 0) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
+            outer = ceil_log2(nd_bis) + 1;                            // :500
+        }
+        // basin labels: basin_id_init + propagate_basin on rec__ = rec_ (:507-511)
+        if (!nonlocal) {
+            PFF_TRY(tile_resolve(rec__, bid, g, w, par, grid, st));
+        } else {
+            PFF_TRY(launch_basin_init(bid, g, st));
             PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-            PFF_CUDA(cudaMemsetAsync(cflags, 0, sizeof(int) * 64, st));
-            for (int r = 0; r < carve_rounds; ++r) {
-                { k_carve_it1<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
-                { k_carve_it2<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
+            PFF_TRY(run_labels(bid, rec__, g, w.ctr + 128, st));
+        }
+        ++n_outer;
+        if (nd_bis == 0) break;  // :512-514
+        // ---- saddlesort (:520), list driven ----
+        if (it == 0) {
+            { k_basin_arrays_init<<<div_up(N + 1, B), B, 0, st>>>(sad, out, basin_saddlenode, w.inv, N + 1); count_launch(); }
+        } else {
+            // the previous saddlesort wrote only the entries of its pits (a superset of the current pits) and 0
+            { k_basin_reset_list<<<grid, B, 0, st>>>(sad, out, basin_saddlenode, w.inv, w.pits[par ^ 1],
+                                                     w.ctr + 16 * (par ^ 1)); count_launch(); }
+        }
+        PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 4 * sizeof(int), st));
+        PFF_MODE_DISPATCH(bound_mode, l_saddle_lists, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z, g,
+                          w.pits[par], np, w.blist, w.ctr + 40, grid, st);
+        if (carve) {
+            // ---- reroute_carve (:405-438) ----
+            PFF_CUDA(cudaMemsetAsync(tag, 0, (size_t)N, st));
+            PFF_CUDA(cudaMemsetAsync(tag_, 0, (size_t)N, st));
+            if (!nonlocal) {
+                // rec == rec_ here; rec__ holds the tile terminals of rec_
+                { k_carve_segments<<<grid, B, 0, st>>>(basin_saddlenode, rec_, rec__, w.pits[par], np, N, w.segs,
+                                                       w.ctr + 41, N, w.ctr + 43); count_launch(); }
+                { k_carve_walk<<<grid, B, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, w.mods,
+                                                   w.ctr + 42, N, w.ctr + 43); count_launch(); }
+                { k_carve_link_list<<<grid, B, 0, st>>>(rec, basin_saddlenode, out, w.pits[par], np, N, w.mods,
+                                                        w.ctr + 42, N, w.ctr + 43); count_launch(); }
+                { k_apply_mods<<<grid, B, 0, st>>>(rec_, w.mods, w.ctr + 42, N); count_launch(); }
+            } else {
+                // general receivers: the reference's tag propagation by pointer jumping
+                { k_carve_tag_saddles<<<nbk, B, 0, st>>>(basin_saddlenode, tag, N); count_launch(); }
+                PFF_CUDA(cudaMemcpyAsync(tag_, tag, (size_t)N, cudaMemcpyDeviceToDevice, st));
+                PFF_CUDA(cudaMemcpyAsync(rec, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+                PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+                int *cflags = w.ctr + 192;
+                PFF_CUDA(cudaMemsetAsync(cflags, 0, sizeof(int) * 64, st));
+                const int carve_rounds = ceil_log2(N) + 2;
+                for (int r = 0; r < carve_rounds; ++r) {
+                    { k_carve_it1<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
+                    { k_carve_it2<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
+                }
+                PFF_CUDA(cudaMemcpyAsync(rec, rec__, nb4, cudaMemcpyDeviceToDevice, st));
+                { k_carve_reverse<<<nbk, B, 0, st>>>(rec, rec__, tag, N); count_launch(); }
+                { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec, basin_saddlenode, out, N, 0); count_launch(); }
+                PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :526
             }
-            PFF_CUDA(cudaMemcpyAsync(rec, rec__, nb4, cudaMemcpyDeviceToDevice, st));
-            { k_carve_reverse<<<nbk, B, 0, st>>>(rec, rec__, tag, N); count_launch(); }
-            { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec, basin_saddlenode, out, N, 0); count_launch(); }
-            PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :526
         } else {
             { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec_, basin_saddlenode, out, N, 1); count_launch(); }  // :529
         }
         PFF_TRY(check_cuda("pff_reroute_flow"));
     }
+    int err = 0;
+    PFF_CUDA(cudaMemcpyAsync(&err, w.ctr + 43, sizeof(int), cudaMemcpyDeviceToHost, st));
     PFF_TRY(launch_basin_init(bid, g, st));  // :537
+    PFF_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        set_error("pff_reroute_flow: carve walk exceeded its bounds (receiver cycle?)");
+        return PFF_ERR_NOCONV;
+    }
     if (n_outer_out) *n_outer_out = n_outer;
     return check_cuda("pff_reroute_flow");
 }

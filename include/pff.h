@@ -74,10 +74,19 @@ int pff_fuse(float *A, const int32_t *src, const float *B, int iteration, int N,
  *   Q      in: per-cell seed (value*dx^2, 1, or per-cell weights); out: upstream sum,
  *          bit-identical to the reference's f32 rake-and-compress result
  *   counts out (optional, may be NULL): exact uint32 upstream cell counts
- * workspace: pff_accumulate_workspace_bytes(N) bytes of device scratch. */
+ * workspace: pff_accumulate_workspace_bytes(N) bytes of device scratch.
+ * A node with more than 4 donors (only jump rerouting can produce one; the
+ * reference's slots overflow there, downstream_propag.py:94-96) is reported as
+ * PFF_ERR_ARG.  Synchronizes `stream` once at the end to read that check. */
 size_t pff_accumulate_workspace_bytes(int N);
 int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *counts, int N, void *workspace,
                    size_t workspace_bytes, void *stream);
+/* Same, with the grid given: donor lists are then built by a gather over each
+ * cell's D4 neighbours (no atomics); receivers that are not D4 neighbours are
+ * detected on the device and handled by the general path.  Same results. */
+int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t *counts, int nx, int ny,
+                        int bound_mode, const uint8_t *codes, int N, void *workspace,
+                        size_t workspace_bytes, void *stream);
 
 /* ---- lake / depression rerouting -----------------------------------------------
  * Replaces pyfastflow/flow/lakeflow.py:466-538 reroute_flow(bid, rec, rec_, rec__,

@@ -359,18 +359,17 @@ int orc_accumulate(const int32_t *rcv, float *Q, uint32_t *cnt, int N, int32_t *
 {
     int32_t *dnr = ws, *dnr_ = ws + 4 * (size_t)N, *ndnr = ws + 8 * (size_t)N,
             *ndnr_ = ws + 9 * (size_t)N;
-    int32_t *src = (int32_t *)malloc(sizeof(int32_t) * (size_t)N);
-    float *Q_ = (float *)malloc(sizeof(float) * (size_t)N);
-    uint32_t *c_ = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)N);
-    int32_t *ndnr_c = (int32_t *)malloc(sizeof(int32_t) * (size_t)N);
-    int32_t *ndnrc_ = (int32_t *)malloc(sizeof(int32_t) * (size_t)N);
-    int32_t *dnr_c = (int32_t *)malloc(sizeof(int32_t) * 4 * (size_t)N);
-    int32_t *dnrc_ = (int32_t *)malloc(sizeof(int32_t) * 4 * (size_t)N);
-    int32_t *src_c = (int32_t *)malloc(sizeof(int32_t) * (size_t)N);
+    /* every buffer starts zeroed, as Taichi fields do */
+    int32_t *src = (int32_t *)calloc((size_t)N, sizeof(int32_t));
+    float *Q_ = (float *)calloc((size_t)N, sizeof(float));
+    uint32_t *c_ = (uint32_t *)calloc((size_t)N, sizeof(uint32_t));
+    int32_t *ndnr_c = (int32_t *)calloc((size_t)N, sizeof(int32_t));
+    int32_t *ndnrc_ = (int32_t *)calloc((size_t)N, sizeof(int32_t));
+    int32_t *dnr_c = (int32_t *)calloc(4 * (size_t)N, sizeof(int32_t));
+    int32_t *dnrc_ = (int32_t *)calloc(4 * (size_t)N, sizeof(int32_t));
+    int32_t *src_c = (int32_t *)calloc((size_t)N, sizeof(int32_t));
     const int logn = orc_ceil_log2(N) + 1;
-    memset(ndnr, 0, sizeof(int32_t) * (size_t)N);
-    memset(src, 0, sizeof(int32_t) * (size_t)N);
-    memset(dnr, 0, sizeof(int32_t) * 4 * (size_t)N);
+    memset(ws, 0, sizeof(int32_t) * 10 * (size_t)N);
     orc_rcv2donor(rcv, dnr, ndnr, N);
     if (cnt) {
         memcpy(ndnr_c, ndnr, sizeof(int32_t) * (size_t)N);

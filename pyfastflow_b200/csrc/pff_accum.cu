@@ -153,26 +153,33 @@ struct __align__(16) Pub {
     int d0;
 };
 
-__global__ void k_acc_init(Pub *A, Pub *B, int4 *priv, const float *__restrict__ Q, uint32_t *counts, int N)
+// Fallback path (receivers that are not D4 neighbours): scatter + sort.  Each
+// kernel runs only if *need is set (need == nullptr: always).
+__global__ void k_acc_init(Pub *A, Pub *B, int4 *priv, const float *__restrict__ Q, uint32_t *counts, int N,
+                           const int *need)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N) return;
-    const Pub s{0, Q[t], 1u, -1};
-    A[t] = s;
-    B[t] = s;
-    priv[t] = make_int4(-1, -1, -1, -1);
-    if (counts) counts[t] = 1u;
+    if (need && !*need) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        const Pub s{0, Q[t], 1u, -1};
+        A[t] = s;
+        B[t] = s;
+        priv[t] = make_int4(-1, -1, -1, -1);
+        if (counts) counts[t] = 1u;
+    }
 }
 
-__global__ void k_acc_scatter(const int32_t *__restrict__ rcv, Pub *A, int4 *priv, int N)
+__global__ void k_acc_scatter(const int32_t *__restrict__ rcv, Pub *A, int4 *priv, int N, const int *need,
+                              int *overflow)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= N) return;
-    const int r = rcv[t];
-    if (r == t) return;
-    const int slot = atomicAdd(&A[r].ndnr, 1);
-    if (slot == 0) A[r].d0 = t;
-    else if (slot < 4) reinterpret_cast<int *>(priv + r)[slot - 1] = t;
+    if (need && !*need) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x) {
+        const int r = rcv[t];
+        if (r == t) continue;
+        const int slot = atomicAdd(&A[r].ndnr, 1);
+        if (slot == 0) A[r].d0 = t;
+        else if (slot < 4) reinterpret_cast<int *>(priv + r)[slot - 1] = t;
+        else *overflow = 1;  // more than 4 donors: the reference's slots overflow into the next node's
+    }
 }
 
 // Block-aggregated append of up to two predicates (order kept within a block).
@@ -198,9 +205,13 @@ __device__ __forceinline__ void block_append2(bool pa, bool pf, int t, int *la, 
 // Sort each node's donor slots ascending, copy its public record to the second
 // buffer, and list the nodes that have donors (round-0 active list).
 template <int BS>
-__global__ void __launch_bounds__(BS) k_acc_list0(Pub *A, Pub *B, int4 *priv, int *list, int *nlist, int N)
+__global__ void __launch_bounds__(BS) k_acc_list0(Pub *A, Pub *B, int4 *priv, int *list, int *nlist, int N,
+                                                  const int *need)
 {
-    const int t = blockIdx.x * BS + threadIdx.x;
+    if (need && !*need) return;
+    const int stride = gridDim.x * BS, trips = (N + stride - 1) / stride;
+    for (int k = 0; k < trips; ++k) {
+    const int t = k * stride + blockIdx.x * BS + threadIdx.x;
     int n = 0;
     if (t < N) {
         Pub s = A[t];
@@ -221,6 +232,92 @@ __global__ void __launch_bounds__(BS) k_acc_list0(Pub *A, Pub *B, int4 *priv, in
         if (n > 0) B[t] = s;
     }
     block_append2<BS>(n > 0, false, t, list, nlist, nullptr, nullptr);
+    }
+}
+
+// Gather-form initialisation for D4 receivers: the donors of t are the cells
+// among its grid neighbours and wrap partners whose receiver is t; visiting
+// them in ascending index gives the reference's serial slot order without
+// atomics or a sort.  Builds both public buffers, the private slots, the
+// counts and the round-0 active list in one pass.  Sets *nonlocal if some
+// receiver is not one of these candidates (then the scatter path redoes it).
+template <int MODE, int BS>
+__global__ void __launch_bounds__(BS) k_acc_gather(const int32_t *__restrict__ rcv, Pub *A, Pub *B, int4 *priv,
+                                                   const float *__restrict__ Q, uint32_t *counts, int *list,
+                                                   int *nlist, int *nonlocal, int *overflow, Grid g)
+{
+    const int col = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int row = blockIdx.y * (BS / 32) + (threadIdx.x >> 5);
+    const bool in = col < g.nx && row < g.ny;
+    const int t = row * g.nx + col;
+    int nd = 0;
+    if (in) {
+        const int rt = rcv[t];
+        bool ok = rt == t;
+        int d[4] = {-1, -1, -1, -1};
+        if (MODE != 3) {
+            // the neighbour relation of modes 0-2 is symmetric: the donors of t are
+            // among its own neighbours; sort them ascending (5 compare-swaps)
+            int cn[4];
+            neighbours4<MODE>(g, t, row, col, cn);
+            int c0 = cn[0], c1 = cn[1], c2 = cn[2], c3 = cn[3];
+            // -1 (no neighbour) sorts last
+            auto key = [](int v) { return (unsigned)v; };
+            auto cs = [&](int &a, int &b) { if (key(a) > key(b)) { int x = a; a = b; b = x; } };
+            cs(c0, c1); cs(c2, c3); cs(c0, c2); cs(c1, c3); cs(c1, c2);
+            const int cc[4] = {c0, c1, c2, c3};
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int j = cc[a];
+                if (j < 0 || (a > 0 && j == cc[a - 1])) continue;
+                if (j == rt) ok = true;
+                if (rcv[j] == t) {
+                    if (nd < 4) d[nd] = j;
+                    ++nd;
+                }
+            }
+        } else {
+            int c[8];
+            const int n = donor_candidates(g, t, row, col, c);
+            for (int a = 0; a < n; ++a) {
+                const int j = c[a];
+                if (j == rt) ok = true;
+                if (rcv[j] == t) {
+                    if (nd < 4) d[nd] = j;
+                    ++nd;
+                }
+            }
+        }
+        if (!ok) *nonlocal = 1;
+        if (nd > 4) *overflow = 1;
+        const Pub s{nd, Q[t], 1u, d[0]};
+        A[t] = s;
+        B[t] = s;
+        if (nd >= 2) priv[t] = make_int4(d[1], d[2], d[3], -1);
+        if (counts) counts[t] = 1u;
+    }
+    block_append2<BS>(nd > 0, false, t, list, nlist, nullptr, nullptr);
+}
+
+__global__ void k_acc_fallback_reset(int *nlist, const int *need)
+{
+    if (*need) *nlist = 0;
+}
+
+__device__ __forceinline__ int sel4(int k, int a, int b, int c, int d)
+{
+    return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d));
+}
+__device__ __forceinline__ void set4(int k, int v, int &a, int &b, int &c, int &d)
+{
+    a = k == 0 ? v : a;
+    b = k == 1 ? v : b;
+    c = k == 2 ? v : c;
+    d = k == 3 ? v : d;
+}
+__device__ __forceinline__ Pub pick4(int q, const Pub &a, const Pub &b, const Pub &c, const Pub &d)
+{
+    return q == 0 ? a : (q == 1 ? b : (q == 2 ? c : d));
 }
 
 // One round.  Items [0, nA) are active nodes, [nA, nA+nF) nodes that finished in
@@ -248,18 +345,29 @@ __global__ void __launch_bounds__(BS) k_acc_round(const Pub *__restrict__ cur, P
             int todo = s.ndnr;
             int own[4] = {s.d0, -1, -1, -1};
             if (todo > 1) {
-                const int4 q = priv[t];
-                own[1] = q.x; own[2] = q.y; own[3] = q.z;
+                const int4 pq = priv[t];
+                own[1] = pq.x; own[2] = pq.y; own[3] = pq.z;
             }
-            int donors[4] = {-1, -1, -1, -1};
+            // Every donor state this round can need is one of the start-of-round
+            // slots: load them all up front (independent loads).  The reference's
+            // swap-remove scan (downstream_propag.py:187-220) then runs on
+            // registers: slot k holds donor w_k whose preloaded state is q_k.
+            Pub P0 = s, P1 = s, P2 = s, P3 = s;
+            if (todo > 0) P0 = cur[own[0]];
+            if (todo > 1) P1 = cur[own[1]];
+            if (todo > 2) P2 = cur[own[2]];
+            if (todo > 3) P3 = cur[own[3]];
+            int w0 = own[0], w1 = own[1], w2 = own[2], w3 = own[3];
+            int q0 = 0, q1 = 1, q2 = 2, q3 = 3;
             bool worked = false;
             float padd = 0.f;
             uint32_t cadd = 0;
             int i = 0;
-            while (i < todo && i < 4) {
-                if (donors[i] == -1) donors[i] = own[i];
-                const int did = donors[i];
-                const Pub ds = cur[did];
+#pragma unroll
+            for (int step = 0; step < 8; ++step) {  // each step advances i or removes a donor
+                if (i >= todo || i >= 4) break;
+                const int q = sel4(i, q0, q1, q2, q3);
+                const Pub ds = pick4(q, P0, P1, P2, P3);
                 if (ds.ndnr <= 1) {
                     if (!worked) { padd = s.p; cadd = s.c; }
                     worked = true;
@@ -267,14 +375,19 @@ __global__ void __launch_bounds__(BS) k_acc_round(const Pub *__restrict__ cur, P
                     cadd += ds.c;
                     if (ds.ndnr == 0) {
                         --todo;
-                        if (todo > i && todo < 4) donors[i] = own[todo];
-                        --i;
+                        if (todo > i && todo < 4) {
+                            set4(i, sel4(todo, own[0], own[1], own[2], own[3]), w0, w1, w2, w3);
+                            set4(i, todo, q0, q1, q2, q3);
+                        }
                     } else {
-                        donors[i] = ds.d0;
+                        set4(i, ds.d0, w0, w1, w2, w3);
+                        ++i;
                     }
+                } else {
+                    ++i;
                 }
-                ++i;
             }
+            const int donors[4] = {w0, w1, w2, w3};
             if (last) {
                 Q[t] = s.p;
                 if (counts) counts[t] = s.c;
@@ -303,6 +416,15 @@ __global__ void __launch_bounds__(BS) k_acc_round(const Pub *__restrict__ cur, P
 __global__ void k_acc_reset_counts(int *c, int n)
 {
     if (threadIdx.x < n) c[threadIdx.x] = 0;
+}
+__global__ void k_acc_fill_one(int *c) { *c = 1; }
+
+template <int MODE>
+static void l_acc_gather(const int32_t *rcv, Pub *A, Pub *B, int4 *priv, const float *Q, uint32_t *counts, int *list,
+                         int *nlist, int *nonlocal, int *overflow, const Grid &g, cudaStream_t st)
+{
+    dim3 gr(div_up(g.nx, 32), div_up(g.ny, 8));
+    { k_acc_gather<MODE, 256><<<gr, 256, 0, st>>>(rcv, A, B, priv, Q, counts, list, nlist, nonlocal, overflow, g); count_launch(); }
 }
 
 }  // namespace pff
@@ -355,7 +477,20 @@ extern "C" size_t pff_accumulate_workspace_bytes(int N)
 extern "C" int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *counts, int N, void *workspace,
                               size_t workspace_bytes, void *stream)
 {
+    return pff_accumulate_grid(receivers, Q, counts, 0, 0, 0, nullptr, N, workspace, workspace_bytes, stream);
+}
+
+extern "C" int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t *counts, int nx, int ny, int mode,
+                                   const uint8_t *codes, int N, void *workspace, size_t workspace_bytes, void *stream)
+{
     clear_error();
+    if (nx > 0) {
+        PFF_TRY(check_grid(nx, ny, mode, codes));
+        if (nx * ny != N) {
+            set_error("pff_accumulate_grid: N != nx*ny");
+            return PFF_ERR_ARG;
+        }
+    }
     if (N <= 0 || !receivers || !Q || 4LL * N >= (1LL << 31)) {
         set_error("pff_accumulate: bad arguments");
         return PFF_ERR_ARG;
@@ -373,16 +508,25 @@ extern "C" int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *coun
     int *lA0 = cv.take<int>(N), *lA1 = cv.take<int>(N), *lF0 = cv.take<int>(N), *lF1 = cv.take<int>(N);
     int *ctr = cv.take<int>(64);  // [2*r] active count, [2*r+1] finished count, by round parity
     constexpr int BS = 256;
-    const int nb = div_up(N, BS);
     const int logn = ceil_log2(N) + 1;  // flowfields.py:272
     { k_acc_reset_counts<<<1, 64, 0, st>>>(ctr, 64); count_launch(); }
-    { k_acc_init<<<nb, BS, 0, st>>>(A, B, priv, Q, counts, N); count_launch(); }
-    { k_acc_scatter<<<nb, BS, 0, st>>>(receivers, A, priv, N); count_launch(); }
-    { k_acc_list0<BS><<<nb, BS, 0, st>>>(A, B, priv, lA0, ctr + 0, N); count_launch(); }
+    int *nonlocal = ctr + 63, *overflow = ctr + 62;
+    if (nx > 0) {
+        Grid g{nx, ny, mode, codes};
+        PFF_MODE_DISPATCH(mode, l_acc_gather, receivers, A, B, priv, Q, counts, lA0, ctr + 0, nonlocal, overflow, g,
+                          st);
+    } else {
+        { k_acc_fill_one<<<1, 1, 0, st>>>(nonlocal); count_launch(); }
+    }
+    // receivers that are not D4 neighbours (or no grid given): scatter path
+    { k_acc_fallback_reset<<<1, 1, 0, st>>>(ctr + 0, nonlocal); count_launch(); }
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = nsm * 8;
+    { k_acc_init<<<grid, BS, 0, st>>>(A, B, priv, Q, counts, N, nonlocal); count_launch(); }
+    { k_acc_scatter<<<grid, BS, 0, st>>>(receivers, A, priv, N, nonlocal, overflow); count_launch(); }
+    { k_acc_list0<BS><<<grid, BS, 0, st>>>(A, B, priv, lA0, ctr + 0, N, nonlocal); count_launch(); }
     Pub *bufs[2] = {A, B};
     int *la[2] = {lA0, lA1}, *lf[2] = {lF0, lF1};
     for (int it = 0; it <= logn; ++it) {
@@ -394,5 +538,14 @@ extern "C" int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *coun
         { k_acc_round<BS><<<grid, BS, 0, st>>>(bufs[a], bufs[b], priv, la[a], na_in, lf[a], nf_in, la[b], na_out,
                                                lf[b], nf_out, Q, counts, it, it == logn); count_launch(); }
     }
-    return check_cuda("pff_accumulate");
+    PFF_TRY(check_cuda("pff_accumulate"));
+    int over = 0;
+    PFF_CUDA(cudaMemcpyAsync(&over, overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PFF_CUDA(cudaStreamSynchronize(st));
+    if (over) {
+        set_error("pff_accumulate: a node has more than 4 donors (possible only after jump rerouting); "
+                  "the reference's donor slots overflow there and this case is not supported");
+        return PFF_ERR_ARG;
+    }
+    return PFF_OK;
 }

@@ -123,6 +123,19 @@ __device__ __forceinline__ bool can_leave(const Grid &g, int i, int row, int col
     return e == 1 || e == 3 || e == 4 || e == 5 || e == 6 || e == 8;
 }
 
+// All four neighours of (row, col); interior cells of modes 0-2 (the bulk of
+// any grid) skip the edge classification.
+template <int MODE>
+__device__ __forceinline__ void neighbours4(const Grid &g, int i, int row, int col, int (&j)[4])
+{
+    if (MODE != 3 && row > 0 && row < g.ny - 1 && col > 0 && col < g.nx - 1) {
+        j[0] = i - g.nx; j[1] = i - 1; j[2] = i + 1; j[3] = i + g.nx;
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) j[k] = neighbour<MODE>(g, i, row, col, k);
+}
+
 template <int MODE>
 __device__ __forceinline__ bool can_leave_i(const Grid &g, int i)
 {
@@ -150,6 +163,32 @@ __host__ __device__ __forceinline__ float key_value(long long k)
     const uint32_t hi = (uint32_t)((unsigned long long)k >> 32);
     const uint32_t u = (hi & 0x80000000u) ? ((~hi) | 0x80000000u) : hi;
     return u2f(u);
+}
+
+// Candidate donors of j: the grid-adjacent cells and the wrap partners across
+// opposite edges (every neighbour relation of every mode is among these).
+__device__ __forceinline__ int donor_candidates(const Grid &g, int j, int row, int col, int *c)
+{
+    int n = 0;
+    const int nx = g.nx, ny = g.ny;
+    if (row > 0) c[n++] = j - nx;
+    if (col > 0) c[n++] = j - 1;
+    if (col < nx - 1) c[n++] = j + 1;
+    if (row < ny - 1) c[n++] = j + nx;
+    if (col == 0) c[n++] = j + nx - 1;
+    if (col == nx - 1) c[n++] = j - nx + 1;
+    if (row == 0) c[n++] = j + nx * (ny - 1);
+    if (row == ny - 1) c[n++] = j - nx * (ny - 1);
+    // ascending, without duplicates
+    for (int a = 1; a < n; ++a) {
+        int x = c[a], b = a - 1;
+        while (b >= 0 && c[b] > x) { c[b + 1] = c[b]; --b; }
+        c[b + 1] = x;
+    }
+    int m = 0;
+    for (int a = 0; a < n; ++a)
+        if (m == 0 || c[m - 1] != c[a]) c[m++] = c[a];
+    return m;
 }
 
 // dispatch a templated launcher on the boundary mode

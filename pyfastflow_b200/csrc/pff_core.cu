@@ -63,9 +63,11 @@ __global__ void __launch_bounds__(256) k_receivers(const float *__restrict__ z, 
     const float zi = z[i];
     int r = i;
     float sr = 0.f;
+    int js[4];
+    neighbours4<MODE>(g, i, row, col, js);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const int j = neighbour<MODE>(g, i, row, col, k);
+        const int j = js[k];
         if (j != -1) {
             const float tsr = __fdiv_rn(__fsub_rn(zi, __ldg(z + j)), dx);
             if (tsr > sr) { sr = tsr; r = j; }

@@ -48,41 +48,17 @@ __global__ void __launch_bounds__(256) k_diffuse_weights(const float *__restrict
     const float zi = zh[i];
     float s[4];
     float sums = 0.f;
+    int js[4];
+    neighbours4<MODE>(g, i, row, col, js);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const int j = neighbour<MODE>(g, i, row, col, k);
+        const int j = js[k];
         s[k] = (j != -1) ? fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zh[j]), dx)) : 0.f;
         sums = __fadd_rn(sums, s[k]);  // j == -1 adds max(0, 0) = 0
     }
     if (sums == 0.f) { issrc[i] = 0; return; }
     issrc[i] = 1;
     w[i] = make_float4(__fdiv_rn(s[0], sums), __fdiv_rn(s[1], sums), __fdiv_rn(s[2], sums), __fdiv_rn(s[3], sums));
-}
-
-// Candidate donors of j: the grid-adjacent cells and the wrap partners across
-// opposite edges (every neighbour relation of every mode is among these).
-__device__ __forceinline__ int diffuse_candidates(const Grid &g, int j, int row, int col, int *c)
-{
-    int n = 0;
-    const int nx = g.nx, ny = g.ny;
-    if (row > 0) c[n++] = j - nx;
-    if (col > 0) c[n++] = j - 1;
-    if (col < nx - 1) c[n++] = j + 1;
-    if (row < ny - 1) c[n++] = j + nx;
-    if (col == 0) c[n++] = j + nx - 1;
-    if (col == nx - 1) c[n++] = j - nx + 1;
-    if (row == 0) c[n++] = j + nx * (ny - 1);
-    if (row == ny - 1) c[n++] = j - nx * (ny - 1);
-    // ascending, without duplicates
-    for (int a = 1; a < n; ++a) {
-        int x = c[a], b = a - 1;
-        while (b >= 0 && c[b] > x) { c[b + 1] = c[b]; --b; }
-        c[b + 1] = x;
-    }
-    int m = 0;
-    for (int a = 0; a < n; ++a)
-        if (m == 0 || c[m - 1] != c[a]) c[m++] = c[a];
-    return m;
 }
 
 // One sweep in gather form: temp[j] = P*dx^2 + sum over sources i ascending, then
@@ -97,7 +73,7 @@ __global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__
     if (col >= g.nx || row >= g.ny) return;
     const int j = row * g.nx + col;
     int c[8];
-    const int n = diffuse_candidates(g, j, row, col, c);
+    const int n = donor_candidates(g, j, row, col, c);
     float acc = prec_dx2;
     for (int a = 0; a < n; ++a) {
         const int i = c[a];

@@ -9,6 +9,7 @@
 //   - saddlesort pass 5: the serial in-place result, computed as snapshot
 //     decisions plus the one basin whose serial outcome can differ
 //     (k_saddle_p5_serial_fix).
+#include <cooperative_groups.h>
 #include <cub/block/block_scan.cuh>
 #include "pff_internal.h"
 #include "pff_tiles.cuh"
@@ -285,9 +286,13 @@ __global__ void k_carve_link_outlets(int32_t *rec, const int32_t *__restrict__ s
 // Pass B: pointer jumping on R over border cells only (a few rounds).
 // Pass L: bid[i] = label of root(i) = Rget(J[i]).
 
+// R is defined at every root (R[x] = x) and every tile-border cell (its root once
+// resolved) -- exactly the cells J can point at.
 __device__ __forceinline__ int r_get(const int32_t *R, int nx, int ny, int x)
 {
-    return is_tile_border_i(nx, ny, x) ? R[x] : x;
+    (void)nx;
+    (void)ny;
+    return R[x];
 }
 
 template <int BS>
@@ -304,38 +309,36 @@ __device__ __forceinline__ void block_append(bool pred, int val, int *list, int 
     __syncthreads();
 }
 
-// info[0] pits, info[1] border cells, info[2] set if some exit target is not a
-// tile-border cell (receivers that are not D4 neighbours)
+// info[0] pits, info[2] set if some exit target is not a tile-border cell
+// (receivers that are not D4 neighbours)
 template <int MODE>
 __global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *__restrict__ rec, int32_t *J, int32_t *R,
-                                                                int *pits, int *borders, int *info, Grid g)
+                                                                int *pits, int *info, Grid g)
 {
     __shared__ int p[TILE_CELLS];
     __shared__ int ext[TILE_CELLS];
     const int nx = g.nx, ny = g.ny;
-    const int tx = blockIdx.x, ty = blockIdx.y;
-    const int col0 = tx * TILE_W, row0 = ty * TILE_H;
+    const int col0 = blockIdx.x * TILE_W, row0 = blockIdx.y * TILE_H;
     const int w = min(TILE_W, nx - col0), h = min(TILE_H, ny - row0);
-    int gi[TILE_PER_THREAD];
 #pragma unroll
     for (int k = 0; k < TILE_PER_THREAD; ++k) {
         const int c = threadIdx.x + k * TILE_THREADS;
         const int lx = c % TILE_W, ly = c / TILE_W;
-        const bool valid = lx < w && ly < h;
-        const int i = valid ? (row0 + ly) * nx + col0 + lx : -1;
-        gi[k] = i;
         int pc = c, e = -2;
-        if (valid) {
+        if (lx < w && ly < h) {
+            const int i = (row0 + ly) * nx + col0 + lx;
             const int r = rec[i];
             if (r == i) {
                 e = -1;
             } else {
-                const int rr = r / nx, rc = r - rr * nx;
-                if (rr >= row0 && rr < row0 + h && rc >= col0 && rc < col0 + w) {
-                    pc = (rr - row0) * TILE_W + (rc - col0);
-                } else {
-                    e = r;
-                }
+                int rly, rlx;
+                if (r == i - 1) { rly = ly; rlx = lx - 1; }
+                else if (r == i + 1) { rly = ly; rlx = lx + 1; }
+                else if (r == i - nx) { rly = ly - 1; rlx = lx; }
+                else if (r == i + nx) { rly = ly + 1; rlx = lx; }
+                else { const int rr = r / nx; rly = rr - row0; rlx = r - rr * nx - col0; }
+                if (rly >= 0 && rly < h && rlx >= 0 && rlx < w) pc = rly * TILE_W + rlx;
+                else e = r;
             }
         }
         p[c] = pc;
@@ -354,40 +357,55 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *_
         }
         if (!__syncthreads_or(ch)) break;
     }
+    bool nonlocal = false;
 #pragma unroll
     for (int k = 0; k < TILE_PER_THREAD; ++k) {
         const int c = threadIdx.x + k * TILE_THREADS;
-        const int i = gi[k];
-        bool pit = false, border = false;
-        if (i >= 0) {
+        const int lx = c % TILE_W, ly = c / TILE_W;
+        bool pit = false;
+        int i = -1;
+        if (lx < w && ly < h) {
+            i = (row0 + ly) * nx + col0 + lx;
             const int t = p[c];
             const int e = ext[t];
             const int j = (e == -1) ? (row0 + t / TILE_W) * nx + col0 + (t % TILE_W) : e;
             J[i] = j;
-            const int lx = c % TILE_W, ly = c / TILE_W;
-            border = lx == 0 || ly == 0 || lx == w - 1 || ly == h - 1;
-            if (border) R[i] = j;
-            if (e >= 0 && !is_tile_border_i(nx, ny, e)) info[2] = 1;  // receivers are not D4
+            if (lx == 0 || ly == 0 || lx == w - 1 || ly == h - 1 || ext[c] == -1) R[i] = j;
+            if (ext[c] >= 0 && !is_tile_border_i(nx, ny, ext[c])) nonlocal = true;
             pit = ext[c] == -1 && !can_leave<MODE>(g, i, row0 + ly, col0 + lx);
         }
-        block_append<TILE_THREADS>(pit, i, pits, info + 0);
-        block_append<TILE_THREADS>(border, i, borders, info + 1);
+        const unsigned m = __ballot_sync(0xffffffffu, pit);
+        if (m) {
+            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(info, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (pit) pits[base + __popc(m & ((1u << lane) - 1u))] = i;
+        }
     }
+    if (nonlocal) info[2] = 1;
 }
 
-__global__ void __launch_bounds__(256) k_border_jump(int32_t *R, const int *__restrict__ borders, const int *nb,
-                                                     int nx, int ny, int r, int *flags)
+// Pointer jumping on R over all border cells, every round in one cooperative
+// launch (grid-wide barrier between rounds); stops after a round with no change.
+__global__ void __launch_bounds__(256) k_border_jump_coop(int32_t *R, int nx, int ny, int ntx, long long nslots,
+                                                          int *flags)
 {
-    if (r > 0 && *(volatile int *)(flags + r - 1) == 0) return;
-    const int n = *nb;
-    bool ch = false;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int e = borders[k];
-        const int x = R[e];
-        const int y = r_get(R, nx, ny, x);
-        if (y != x) { R[e] = y; ch = true; }
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int r = 0; r < 32; ++r) {
+        bool ch = false;
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nslots; k += stride) {
+            const int e = border_cell(nx, ny, ntx, k);
+            if (e < 0) continue;
+            const int x = R[e];
+            const int y = r_get(R, nx, ny, x);
+            if (y != x) { R[e] = y; ch = true; }
+        }
+        if (__syncthreads_or(ch) && threadIdx.x == 0) flags[r] = 1;
+        grid.sync();
+        if (*(volatile int *)(flags + r) == 0) break;
     }
-    if (__syncthreads_or(ch) && threadIdx.x == 0) flags[r] = 1;
 }
 
 template <int MODE>
@@ -435,11 +453,11 @@ __global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restri
         } else {
             const int bi = bid[i];
             int js[4];
+            neighbours4<MODE>(g, i, row, col, js);
             float zn = 1e9f;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const int j = neighbour<MODE>(g, i, row, col, k);
-                js[k] = j;
+                const int j = js[k];
                 if (j != -1 && bid[j] != bi) { border = true; zn = fminf(zn, z[j]); }
             }
             is_border[i] = border;
@@ -657,11 +675,11 @@ static void l_saddle(const int32_t *bid, uint8_t *isb, float *zp, long long *sad
 }
 
 template <int MODE>
-static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pits, int *borders, int *info,
-                            const Grid &g, cudaStream_t st)
+static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pits, int *info, const Grid &g,
+                            cudaStream_t st)
 {
     dim3 gr(div_up(g.nx, TILE_W), div_up(g.ny, TILE_H));
-    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, borders, info, g); count_launch(); }
+    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g); count_launch(); }
 }
 template <int MODE>
 static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, cudaStream_t st)
@@ -774,7 +792,7 @@ extern "C" int pff_saddlesort(const int32_t *bid, uint8_t *is_border, float *z_p
 extern "C" size_t pff_reroute_workspace_bytes(int N)
 {
     const size_t n = (size_t)N;
-    return Carver::round(n + 1) + Carver::round(4 * n) * 6 + Carver::round(8 * n) + Carver::round(sizeof(int) * 512) +
+    return Carver::round(n + 1) + Carver::round(4 * n) * 5 + Carver::round(8 * n) + Carver::round(sizeof(int) * 512) +
            4096;
 }
 
@@ -784,8 +802,8 @@ struct RerouteWs {
     uint8_t *inv;
     int32_t *R;
     int *pits[2];
-    int *borders, *blist, *segs, *mods;
-    int *ctr;  // [16*p + 0] pits, +1 borders, +2 non-D4 flag (parity p); [40] nblist, [41] nsegs, [42] nmods,
+    int *blist, *segs, *mods;
+    int *ctr;  // [16*p + 0] pits, +2 non-D4 flag (parity p); [40] nblist, [41] nsegs, [42] nmods,
                // [43] error; [64..127] border-jump round flags; [128..191] label round flags
 };
 
@@ -797,7 +815,6 @@ static RerouteWs carve_ws(void *workspace, size_t bytes, int N)
     w.R = cv.take<int32_t>(N);
     w.pits[0] = cv.take<int>(N);
     w.pits[1] = cv.take<int>(N);
-    w.borders = cv.take<int>(N);
     w.blist = cv.take<int>(N);
     w.segs = cv.take<int>(N);
     w.mods = cv.take<int>(2 * (size_t)N);
@@ -813,7 +830,7 @@ static int tile_pass(const int32_t *rec, int32_t *Jbuf, const Grid &g, RerouteWs
 {
     int *info = w.ctr + 16 * parity;
     PFF_CUDA(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
-    PFF_MODE_DISPATCH(g.mode, l_tile_terminal, rec, Jbuf, w.R, w.pits[parity], w.borders, info, g, st);
+    PFF_MODE_DISPATCH(g.mode, l_tile_terminal, rec, Jbuf, w.R, w.pits[parity], info, g, st);
     int h[4];
     PFF_CUDA(cudaMemcpyAsync(h, info, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PFF_CUDA(cudaStreamSynchronize(st));
@@ -827,12 +844,24 @@ static int tile_pass(const int32_t *rec, int32_t *Jbuf, const Grid &g, RerouteWs
 static int tile_resolve(const int32_t *Jbuf, int32_t *bid, const Grid &g, RerouteWs &w, int parity, int grid,
                         cudaStream_t st)
 {
-    int *info = w.ctr + 16 * parity;
+    (void)parity;
     int *flags = w.ctr + 64;
     PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
-    for (int r = 0; r < 32; ++r) {
-        { k_border_jump<<<grid, 256, 0, st>>>(w.R, w.borders, info + 1, g.nx, g.ny, r, flags); count_launch(); }
+    static int coop_blocks = 0;
+    if (!coop_blocks) {
+        int dev = 0, nsm = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_border_jump_coop, 256, 0);
+        coop_blocks = nsm * (per < 4 ? per : 4);
     }
+    int nx = g.nx, ny = g.ny, ntx = div_up(g.nx, TILE_W);
+    long long nslots = (long long)ntx * div_up(g.ny, TILE_H) * BORDER_SLOTS;
+    int32_t *R = w.R;
+    void *args[] = {&R, &nx, &ny, &ntx, &nslots, &flags};
+    PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_border_jump_coop, coop_blocks, 256, args, 0, st));
+    count_launch();
+    (void)grid;
     PFF_MODE_DISPATCH(g.mode, l_labels_final, Jbuf, w.R, bid, g, st);
     return check_cuda("tile_resolve");
 }

@@ -138,8 +138,9 @@ class FlowRouter:
 
     def _accumulate(self, counts: bool = True):
         wp, wn = self._ws_acc.get(_lib.load().pff_accumulate_workspace_bytes(self.N), self.device)
-        _lib.call("pff_accumulate", self.receivers.data_ptr(), self.Q.data_ptr(),
-                  self.counts.data_ptr() if counts else None, self.N, wp, wn, _dev.stream())
+        _lib.call("pff_accumulate_grid", self.receivers.data_ptr(), self.Q.data_ptr(),
+                  self.counts.data_ptr() if counts else None, self.nx, self.ny, self.mode, self._codes(), self.N,
+                  wp, wn, _dev.stream())
 
     def accumulate_constant_Q(self, value, area=True, counts=True):
         """flowfields.py:254-292: Q = value*dx^2 (area) or value per cell,

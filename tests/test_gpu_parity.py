@@ -139,7 +139,7 @@ def test_reroute(orc, cuda, mode, carve):
     torch = cuda
     from pyfastflow_b200 import flow
 
-    for kind, (nx, ny) in [("spectral", (211, 173)), ("int", (64, 48))]:
+    for kind, (nx, ny) in [("spectral", (211, 173)), ("int", (64, 48)), ("int", (9, 7)), ("uniform", (130, 66))]:
         g = Grid(orc, torch, nx, ny, mode, seed=7)
         z = make_case(kind, nx, ny, seed=31 + mode)
         set_constants(g, 10.0)
@@ -242,3 +242,48 @@ def test_routing_plain_512_bit_exact(orc, cuda):
     cnt = orc.topo_accumulate(rcv)
     assert np.array_equal(router.get_counts().ravel(), cnt)
     assert np.array_equal(router.get_Q().ravel(), cnt.astype(np.float32))
+
+
+@pytest.mark.parametrize("grid_given", [True, False])
+def test_accumulate_general_forest(orc, cuda, grid_given):
+    """Receivers that are not D4 neighbours (an arbitrary forest) take the
+    scatter path; D4 receivers take the gather path; both bit-exact."""
+    torch = cuda
+    from pyfastflow_b200 import _dev, _lib
+
+    rng = np.random.default_rng(12)
+    nx, ny = 150, 120
+    N = nx * ny
+    forests = []
+    # random forest, parent index below the child's, at most 4 donors per node
+    rcv = np.arange(N, dtype=np.int32)
+    nchild = np.zeros(N, np.int32)
+    for i in range(1, N):
+        if rng.random() < 0.03:
+            continue
+        for _ in range(8):
+            p = int(rng.integers(max(0, i - 5000), i))
+            if nchild[p] < 4:
+                rcv[i] = p
+                nchild[p] += 1
+                break
+    forests.append(rcv)
+    z = make_case("spectral", nx, ny, seed=3)
+    og = orc.Grid(nx, ny, 0)
+    r_d4, _ = orc.compute_receivers(z, og, 10.0)
+    forests.append(orc.reroute_flow(r_d4, z, og)[0])
+    ws = _dev.Scratch()
+    for rcv in forests:
+        w = rng.lognormal(0, 0.5, N).astype(np.float32)
+        Qd = dev(torch, w)
+        cd = torch.zeros(N, dtype=torch.int32, device="cuda")
+        wp, wn = ws.get(_lib.load().pff_accumulate_workspace_bytes(N))
+        if grid_given:
+            _lib.call("pff_accumulate_grid", dev(torch, rcv).data_ptr(), Qd.data_ptr(), cd.data_ptr(), nx, ny, 0,
+                      None, N, wp, wn, _dev.stream())
+        else:
+            _lib.call("pff_accumulate", dev(torch, rcv).data_ptr(), Qd.data_ptr(), cd.data_ptr(), N, wp, wn,
+                      _dev.stream())
+        Qo, co = orc.accumulate(rcv, w)
+        assert np.array_equal(host(cd).view(np.uint32), co)
+        assert np.array_equal(host(Qd).view(np.uint32), Qo.view(np.uint32))

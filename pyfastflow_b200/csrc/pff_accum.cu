@@ -292,9 +292,13 @@ __global__ void __launch_bounds__(BS) k_acc_gather(const int32_t *__restrict__ r
         if (nd > 4) *overflow = 1;
         const Pub s{nd, Q[t], 1u, d[0]};
         A[t] = s;
-        B[t] = s;
+        if (nd == 0) {
+            // leaves: final from the start, in both buffers; active nodes rewrite B
+            // in round 0 and write their counts when they finish
+            B[t] = s;
+            if (counts) counts[t] = 1u;
+        }
         if (nd >= 2) priv[t] = make_int4(d[1], d[2], d[3], -1);
-        if (counts) counts[t] = 1u;
     }
     block_append2<BS>(nd > 0, false, t, list, nlist, nullptr, nullptr);
 }
@@ -325,7 +329,7 @@ __device__ __forceinline__ Pub pick4(int q, const Pub &a, const Pub &b, const Pu
 // round (it == logn) every active node reports its start-of-round value, which
 // is what the reference's fuse(.., logn) selects (downstream_propag.py:59-74).
 template <int BS>
-__global__ void __launch_bounds__(BS) k_acc_round(const Pub *__restrict__ cur, Pub *nxt, int4 *priv,
+__global__ void __launch_bounds__(BS, 5) k_acc_round(const Pub *__restrict__ cur, Pub *nxt, int4 *priv,
                                                   const int *__restrict__ la, const int *nla,
                                                   const int *__restrict__ lf, const int *nlf, int *la2, int *nla2,
                                                   int *lf2, int *nlf2, float *Q, uint32_t *counts, int it, int last)
@@ -527,6 +531,12 @@ extern "C" int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t 
     { k_acc_init<<<grid, BS, 0, st>>>(A, B, priv, Q, counts, N, nonlocal); count_launch(); }
     { k_acc_scatter<<<grid, BS, 0, st>>>(receivers, A, priv, N, nonlocal, overflow); count_launch(); }
     { k_acc_list0<BS><<<grid, BS, 0, st>>>(A, B, priv, lA0, ctr + 0, N, nonlocal); count_launch(); }
+    static int round_blocks = 0;
+    if (!round_blocks) {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_acc_round<BS>, BS, 0);
+        round_blocks = nsm * (per > 0 ? per : 1);
+    }
     Pub *bufs[2] = {A, B};
     int *la[2] = {lA0, lA1}, *lf[2] = {lF0, lF1};
     for (int it = 0; it <= logn; ++it) {
@@ -535,7 +545,7 @@ extern "C" int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t 
         int *na_in = ctr + 4 * a, *nf_in = na_in + 1;
         int *na_out = ctr + 4 * b, *nf_out = na_out + 1;
         PFF_CUDA(cudaMemsetAsync(na_out, 0, 2 * sizeof(int), st));
-        { k_acc_round<BS><<<grid, BS, 0, st>>>(bufs[a], bufs[b], priv, la[a], na_in, lf[a], nf_in, la[b], na_out,
+        { k_acc_round<BS><<<round_blocks, BS, 0, st>>>(bufs[a], bufs[b], priv, la[a], na_in, lf[a], nf_in, la[b], na_out,
                                                lf[b], nf_out, Q, counts, it, it == logn); count_launch(); }
     }
     PFF_TRY(check_cuda("pff_accumulate"));

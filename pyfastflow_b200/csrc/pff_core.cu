@@ -63,14 +63,22 @@ __global__ void __launch_bounds__(256) k_receivers(const float *__restrict__ z, 
     const float zi = z[i];
     int r = i;
     float sr = 0.f;
+    // A drop d can only beat the current best if d exceeds the best drop so far
+    // (division by dx > 0 is monotone), so the IEEE division -- the costly part --
+    // runs only for improving candidates; the comparison is still on the rounded
+    // quotients, as in the reference (ties after rounding keep the earlier k).
+    float dbest = 0.f;
     int js[4];
     neighbours4<MODE>(g, i, row, col, js);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int j = js[k];
         if (j != -1) {
-            const float tsr = __fdiv_rn(__fsub_rn(zi, __ldg(z + j)), dx);
-            if (tsr > sr) { sr = tsr; r = j; }
+            const float d = __fsub_rn(zi, __ldg(z + j));
+            if (d > dbest) {
+                const float tsr = __fdiv_rn(d, dx);
+                if (tsr > sr) { sr = tsr; r = j; dbest = d; }
+            }
         }
     }
     rcv[i] = r;

@@ -311,14 +311,22 @@ __device__ __forceinline__ void block_append(bool pred, int val, int *list, int 
 
 // info[0] pits, info[2] set if some exit target is not a tile-border cell
 // (receivers that are not D4 neighbours)
+// tiles: optional list of tile ids (blockIdx.x indexes it) -- recompute only
+// those tiles; pits: optional (nullptr: no pit list).
 template <int MODE>
 __global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *__restrict__ rec, int32_t *J, int32_t *R,
-                                                                int *pits, int *info, Grid g)
+                                                                int *pits, int *info, Grid g, const int *tiles)
 {
     __shared__ int p[TILE_CELLS];
     __shared__ int ext[TILE_CELLS];
     const int nx = g.nx, ny = g.ny;
-    const int col0 = blockIdx.x * TILE_W, row0 = blockIdx.y * TILE_H;
+    int tx = blockIdx.x, ty = blockIdx.y;
+    if (tiles) {
+        const int ntx = (nx + TILE_W - 1) / TILE_W, t = tiles[blockIdx.x];
+        ty = t / ntx;
+        tx = t - ty * ntx;
+    }
+    const int col0 = tx * TILE_W, row0 = ty * TILE_H;
     const int w = min(TILE_W, nx - col0), h = min(TILE_H, ny - row0);
 #pragma unroll
     for (int k = 0; k < TILE_PER_THREAD; ++k) {
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *_
             J[i] = j;
             if (lx == 0 || ly == 0 || lx == w - 1 || ly == h - 1 || ext[c] == -1) R[i] = j;
             if (ext[c] >= 0 && !is_tile_border_i(nx, ny, ext[c])) nonlocal = true;
-            pit = ext[c] == -1 && !can_leave<MODE>(g, i, row0 + ly, col0 + lx);
+            pit = pits && ext[c] == -1 && !can_leave<MODE>(g, i, row0 + ly, col0 + lx);
         }
         const unsigned m = __ballot_sync(0xffffffffu, pit);
         if (m) {
@@ -480,6 +488,7 @@ __global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restri
             }
         }
     }
+    // one atomic per block: a per-warp atomic on this single counter serialises in L2
     block_append<256>(border && bid[i] != 0, i, blist, nblist);
 }
 
@@ -576,17 +585,51 @@ __global__ void k_saddle_p5_apply_list(long long *saddle, long long *outlet, int
 //     rec_, which stays unchanged until every walk is done.
 // Link: rec[saddle node] = outlet node (:399-403).  Every write to rec is also
 // recorded, then replayed onto rec_ so both end equal, as in the reference.
-__global__ void k_carve_segments(const int32_t *__restrict__ snode, const int32_t *__restrict__ rec0,
-                                 const int32_t *__restrict__ J, const int *__restrict__ pits, const int *np, int N,
-                                 int *segs, int *nsegs, int cap, int *err)
+__device__ __forceinline__ void mark_tile(uint8_t *dirty, int nx, int pos)
+{
+    if (!dirty) return;
+    const int row = pos / nx;
+    dirty[(row / TILE_H) * ((nx + TILE_W - 1) / TILE_W) + (pos - row * nx) / TILE_W] = 1;
+}
+
+// Walk one path segment inside the tile of `start`: tag the cells and reverse the
+// links (rec[next] = cell, :395-397), reading the old receivers from rec0.
+// Returns the first cell outside the tile, or -1 if the segment ends at the pit.
+__device__ __forceinline__ int walk_segment(int start, const int32_t *__restrict__ rec0, int32_t *rec, uint8_t *tag,
+                                            uint8_t *tag_, int nx, uint8_t *dirty)
+{
+    int x = start;
+    for (int step = 0; step < TILE_CELLS + 1; ++step) {
+        tag[x] = 1;
+        tag_[x] = 1;
+        const int nxt = rec0[x];
+        if (nxt == x) return -1;
+        rec[nxt] = x;
+        mark_tile(dirty, nx, nxt);
+        if (!same_tile(nx, nxt, start)) return nxt;
+        x = nxt;
+    }
+    return -1;
+}
+
+// Per basin with a saddle node: walk the first segment (in the saddle node's
+// tile) directly, then hop tile by tile through J and list the later segment
+// starts for k_carve_walk.
+__global__ void k_carve_segments(const int32_t *__restrict__ snode, const int32_t *__restrict__ rec0, int32_t *rec,
+                                 uint8_t *tag, uint8_t *tag_, const int32_t *__restrict__ J,
+                                 const int *__restrict__ pits, const int *np, int N, int nx, int *segs, int *nsegs,
+                                 int cap, int *err, uint8_t *dirty)
 {
     const int n = *np;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int b = pits[k] + 1;
         if (b >= N) continue;
-        int x = snode[b];
-        if (x < 0) continue;
-        for (int step = 0; step < N; ++step) {
+        const int s0 = snode[b];
+        if (s0 < 0) continue;
+        int x = walk_segment(s0, rec0, rec, tag, tag_, nx, dirty);
+        // x is now the first cell outside the saddle node's tile (or -1 at the pit);
+        // J hops from there give every later segment start
+        for (int step = 0; x >= 0 && step < N; ++step) {
             const int slot = atomicAdd(nsegs, 1);
             if (slot < cap) segs[slot] = x;
             else { *err = 1; break; }
@@ -597,31 +640,15 @@ __global__ void k_carve_segments(const int32_t *__restrict__ snode, const int32_
 }
 
 __global__ void k_carve_walk(const int32_t *__restrict__ rec0, int32_t *rec, uint8_t *tag, uint8_t *tag_,
-                             const int *__restrict__ segs, const int *nsegs, int cap, int nx, int *mods, int *nmods,
-                             int mcap, int *err)
+                             const int *__restrict__ segs, const int *nsegs, int cap, int nx, uint8_t *dirty)
 {
     const int n = min(*nsegs, cap);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int start = segs[k];
-        int x = start;
-        for (int step = 0; step < TILE_CELLS + 1; ++step) {
-            tag[x] = 1;
-            tag_[x] = 1;
-            const int nxt = rec0[x];
-            if (nxt == x) break;
-            rec[nxt] = x;
-            const int slot = atomicAdd(nmods, 1);
-            if (slot < mcap) { mods[2 * slot] = nxt; mods[2 * slot + 1] = x; }
-            else *err = 1;
-            if (!same_tile(nx, nxt, start)) break;
-            x = nxt;
-        }
-    }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        walk_segment(segs[k], rec0, rec, tag, tag_, nx, dirty);
 }
 
 __global__ void k_carve_link_list(int32_t *rec, const int32_t *__restrict__ snode, const long long *__restrict__ outlet,
-                                  const int *__restrict__ pits, const int *np, int N, int *mods, int *nmods, int mcap,
-                                  int *err)
+                                  const int *__restrict__ pits, const int *np, int N, uint8_t *dirty, int nx)
 {
     const int n = *np;
     const long long iv = invalid_key();
@@ -632,18 +659,121 @@ __global__ void k_carve_link_list(int32_t *rec, const int32_t *__restrict__ snod
         if (o == iv) continue;
         const int s = snode[b], v = key_index(o);
         rec[s] = v;
-        const int slot = atomicAdd(nmods, 1);
-        if (slot < mcap) { mods[2 * slot] = s; mods[2 * slot + 1] = v; }
-        else *err = 1;
+        mark_tile(dirty, nx, s);
     }
 }
 
-// replay onto rec_; order does not matter: every position is written once
-__global__ void k_apply_mods(int32_t *dst, const int *__restrict__ mods, const int *nmods, int mcap)
+// ---- next iteration's labels without relabelling from scratch ---------------------
+//
+// After the carve, every cell of a basin b with a valid outlet drains through its
+// saddle node into basin bid[outlet node]; nothing else changes.  So the next
+// labels are bid'[i] = final(bid[i]), final = the end of the chain
+// b -> bid[outlet node of b] -> ..., and the next pits are the pits of the
+// basins that had no valid outlet.  fin[] is indexed by basin id.
+__global__ void k_relabel_init(int32_t *fin, const int32_t *__restrict__ bid, const int32_t *__restrict__ snode,
+                               const long long *__restrict__ outlet, const int *__restrict__ pits, const int *np, int N,
+                               int *next_pits, int *next_np, int *odd)
 {
-    const int n = min(*nmods, mcap);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        dst[mods[2 * k]] = mods[2 * k + 1];
+    const int n = *np;
+    const long long iv = invalid_key();
+    if (blockIdx.x == 0 && threadIdx.x == 0) fin[0] = 0;
+    const int n32 = (n + 31) & ~31;  // whole warps iterate together (ballot below)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n32; k += gridDim.x * blockDim.x) {
+        bool keep = false;
+        int p = -1;
+        if (k < n) {
+            p = pits[k];
+            const int b = p + 1;
+            const long long o = (b < N) ? outlet[b] : iv;
+            if (o != iv) {
+                fin[b] = bid[key_index(o)];
+            } else {
+                fin[b] = b;
+                keep = true;
+                if (b < N && snode[b] != -1) *odd = 1;  // path reversed without an outlet link
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (m) {
+            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(next_np, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (keep) next_pits[base + __popc(m & ((1u << lane) - 1u))] = p;
+        }
+    }
+}
+
+// fin[b] = fin[fin[b]] over the pit list, all rounds in one cooperative launch.
+__global__ void __launch_bounds__(256) k_relabel_jump_coop(int32_t *fin, const int *__restrict__ pits, const int *np,
+                                                           int *flags)
+{
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const int n = *np;
+    for (int r = 0; r < 32; ++r) {
+        bool ch = false;
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            const int b = pits[k] + 1;
+            const int x = fin[b];
+            const int y = fin[x];
+            if (y != x) { fin[b] = y; ch = true; }
+        }
+        if (__syncthreads_or(ch) && threadIdx.x == 0) flags[r] = 1;
+        grid.sync();
+        if (*(volatile int *)(flags + r) == 0) break;
+    }
+}
+
+// four cells per thread; label 0 (outlet basins) never changes
+__global__ void __launch_bounds__(256) k_relabel(int32_t *bid, const int32_t *__restrict__ fin, int N, int vec)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = 4 * q;
+    if (vec && i + 3 < N) {
+        int4 b = reinterpret_cast<int4 *>(bid)[q];
+        const int4 o = b;
+        if (b.x) b.x = fin[b.x];
+        if (b.y) b.y = fin[b.y];
+        if (b.z) b.z = fin[b.z];
+        if (b.w) b.w = fin[b.w];
+        if (b.x != o.x || b.y != o.y || b.z != o.z || b.w != o.w) reinterpret_cast<int4 *>(bid)[q] = b;
+    } else {
+        for (int k = i; k < N && k < i + 4; ++k)
+            if (bid[k]) bid[k] = fin[bid[k]];
+    }
+}
+
+__global__ void k_dirty_list(uint8_t *dirty, int ntiles, int *list, int *count)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool d = t < ntiles && dirty[t];
+    if (d) dirty[t] = 0;
+    const unsigned m = __ballot_sync(0xffffffffu, d);
+    if (m) {
+        const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (d) list[base + __popc(m & ((1u << lane) - 1u))] = t;
+    }
+}
+
+// rec_ = rec on the carved cells: every write of the carve (reversed links and
+// saddle links) is at a tagged cell, and rec == rec_ everywhere else.
+__global__ void __launch_bounds__(256) k_sync_tagged(int32_t *rec_, const int32_t *__restrict__ rec,
+                                                     const uint8_t *__restrict__ tag, int N, int vec)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = 4 * q;
+    if (vec && i + 3 < N) {
+        const uchar4 t = reinterpret_cast<const uchar4 *>(tag)[q];
+        if (t.x) rec_[i] = rec[i];
+        if (t.y) rec_[i + 1] = rec[i + 1];
+        if (t.z) rec_[i + 2] = rec[i + 2];
+        if (t.w) rec_[i + 3] = rec[i + 3];
+    } else {
+        for (int k = i; k < N && k < i + 4; ++k)
+            if (tag[k]) rec_[k] = rec[k];
     }
 }
 
@@ -679,7 +809,14 @@ static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pit
                             cudaStream_t st)
 {
     dim3 gr(div_up(g.nx, TILE_W), div_up(g.ny, TILE_H));
-    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g); count_launch(); }
+    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g, nullptr); count_launch(); }
+}
+template <int MODE>
+static void l_tile_terminal_list(const int32_t *rec, int32_t *J, int32_t *R, int *info, const Grid &g,
+                                 const int *tiles, int ntiles, cudaStream_t st)
+{
+    if (ntiles <= 0) return;
+    { k_tile_terminal<MODE><<<ntiles, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles); count_launch(); }
 }
 template <int MODE>
 static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, cudaStream_t st)
@@ -792,19 +929,22 @@ extern "C" int pff_saddlesort(const int32_t *bid, uint8_t *is_border, float *z_p
 extern "C" size_t pff_reroute_workspace_bytes(int N)
 {
     const size_t n = (size_t)N;
-    return Carver::round(n + 1) + Carver::round(4 * n) * 5 + Carver::round(8 * n) + Carver::round(sizeof(int) * 512) +
-           4096;
+    return Carver::round(n + 1) * 2 + Carver::round(4 * (n + 1)) + Carver::round(4 * n) * 6 + Carver::round(8 * n) +
+           Carver::round(sizeof(int) * 512) + 8192;
 }
 
 namespace pff {
 
 struct RerouteWs {
     uint8_t *inv;
-    int32_t *R;
+    int32_t *R, *fin;
+    uint8_t *dirty;
+    int *tiles;
     int *pits[2];
-    int *blist, *segs, *mods;
+    int *blist, *segs;
     int *ctr;  // [16*p + 0] pits, +2 non-D4 flag (parity p); [40] nblist, [41] nsegs, [42] nmods,
-               // [43] error; [64..127] border-jump round flags; [128..191] label round flags
+               // [43] error; [44] dirty tiles; [45] odd carve; [64..127] border-jump round flags;
+               // [128..191] label round flags; [192..255] carve round flags; [256..319] relabel flags
 };
 
 static RerouteWs carve_ws(void *workspace, size_t bytes, int N)
@@ -813,11 +953,13 @@ static RerouteWs carve_ws(void *workspace, size_t bytes, int N)
     RerouteWs w;
     w.inv = cv.take<uint8_t>((size_t)N + 1);
     w.R = cv.take<int32_t>(N);
+    w.fin = cv.take<int32_t>((size_t)N + 1);
+    w.dirty = cv.take<uint8_t>((size_t)N);  // one byte per tile needed; N bytes bounds it
+    w.tiles = cv.take<int>(N);
     w.pits[0] = cv.take<int>(N);
     w.pits[1] = cv.take<int>(N);
     w.blist = cv.take<int>(N);
     w.segs = cv.take<int>(N);
-    w.mods = cv.take<int>(2 * (size_t)N);
     w.ctr = cv.take<int>(512);
     return w;
 }
@@ -900,32 +1042,45 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
 
     PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :491
     PFF_CUDA(cudaMemsetAsync(w.ctr, 0, 512 * sizeof(int), st));
+    const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(ny, TILE_H);
+    PFF_CUDA(cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, st));
     int outer = 0, n_outer = 0;
+    // In carve mode with D4 receivers, labels after iteration 0 come from relabelling
+    // basin ids (k_relabel_*), and tile terminals are recomputed for dirty tiles only.
+    bool incremental = false;
+    int nd_next = 0;
     for (int it = 0;; ++it) {
         if (it > 0 && it >= outer) break;  // :500
         const int par = it & 1;
         int *np = w.ctr + 16 * par;
         int nd_bis = 0, nonlocal = 1;
-        // depression_counter(rec_) (:493, :501), with the pit list
-        if (carve) {
-            PFF_TRY(tile_pass(rec_, rec__, g, w, par, &nd_bis, &nonlocal, st));
+        if (incremental) {
+            nd_bis = nd_next;  // pits left after the previous carve; bid already relabelled
+            nonlocal = 0;
         } else {
-            PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
-            PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);
-            PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
-            PFF_CUDA(cudaStreamSynchronize(st));
+            // depression_counter(rec_) (:493, :501), with the pit list
+            if (carve) {
+                PFF_TRY(tile_pass(rec_, rec__, g, w, par, &nd_bis, &nonlocal, st));
+            } else {
+                PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
+                PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);
+                PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
+                PFF_CUDA(cudaStreamSynchronize(st));
+            }
         }
         if (it == 0) {
             if (nd_bis == 0) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
             outer = ceil_log2(nd_bis) + 1;                            // :500
         }
-        // basin labels: basin_id_init + propagate_basin on rec__ = rec_ (:507-511)
-        if (!nonlocal) {
-            PFF_TRY(tile_resolve(rec__, bid, g, w, par, grid, st));
-        } else {
-            PFF_TRY(launch_basin_init(bid, g, st));
-            PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-            PFF_TRY(run_labels(bid, rec__, g, w.ctr + 128, st));
+        if (!incremental) {
+            // basin labels: basin_id_init + propagate_basin on rec__ = rec_ (:507-511)
+            if (!nonlocal) {
+                PFF_TRY(tile_resolve(rec__, bid, g, w, par, grid, st));
+            } else {
+                PFF_TRY(launch_basin_init(bid, g, st));
+                PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+                PFF_TRY(run_labels(bid, rec__, g, w.ctr + 128, st));
+            }
         }
         ++n_outer;
         if (nd_bis == 0) break;  // :512-514
@@ -933,46 +1088,83 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         if (it == 0) {
             { k_basin_arrays_init<<<div_up(N + 1, B), B, 0, st>>>(sad, out, basin_saddlenode, w.inv, N + 1); count_launch(); }
         } else {
-            // the previous saddlesort wrote only the entries of its pits (a superset of the current pits) and 0
+            // the previous saddlesort wrote only the entries of its pits (a superset of the current ones) and 0
             { k_basin_reset_list<<<grid, B, 0, st>>>(sad, out, basin_saddlenode, w.inv, w.pits[par ^ 1],
                                                      w.ctr + 16 * (par ^ 1)); count_launch(); }
         }
-        PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 4 * sizeof(int), st));
+        PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 6 * sizeof(int), st));
         PFF_MODE_DISPATCH(bound_mode, l_saddle_lists, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z, g,
                           w.pits[par], np, w.blist, w.ctr + 40, grid, st);
-        if (carve) {
-            // ---- reroute_carve (:405-438) ----
-            PFF_CUDA(cudaMemsetAsync(tag, 0, (size_t)N, st));
-            PFF_CUDA(cudaMemsetAsync(tag_, 0, (size_t)N, st));
-            if (!nonlocal) {
-                // rec == rec_ here; rec__ holds the tile terminals of rec_
-                { k_carve_segments<<<grid, B, 0, st>>>(basin_saddlenode, rec_, rec__, w.pits[par], np, N, w.segs,
-                                                       w.ctr + 41, N, w.ctr + 43); count_launch(); }
-                { k_carve_walk<<<grid, B, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, w.mods,
-                                                   w.ctr + 42, N, w.ctr + 43); count_launch(); }
-                { k_carve_link_list<<<grid, B, 0, st>>>(rec, basin_saddlenode, out, w.pits[par], np, N, w.mods,
-                                                        w.ctr + 42, N, w.ctr + 43); count_launch(); }
-                { k_apply_mods<<<grid, B, 0, st>>>(rec_, w.mods, w.ctr + 42, N); count_launch(); }
-            } else {
-                // general receivers: the reference's tag propagation by pointer jumping
-                { k_carve_tag_saddles<<<nbk, B, 0, st>>>(basin_saddlenode, tag, N); count_launch(); }
-                PFF_CUDA(cudaMemcpyAsync(tag_, tag, (size_t)N, cudaMemcpyDeviceToDevice, st));
-                PFF_CUDA(cudaMemcpyAsync(rec, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-                PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-                int *cflags = w.ctr + 192;
-                PFF_CUDA(cudaMemsetAsync(cflags, 0, sizeof(int) * 64, st));
-                const int carve_rounds = ceil_log2(N) + 2;
-                for (int r = 0; r < carve_rounds; ++r) {
-                    { k_carve_it1<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
-                    { k_carve_it2<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
-                }
-                PFF_CUDA(cudaMemcpyAsync(rec, rec__, nb4, cudaMemcpyDeviceToDevice, st));
-                { k_carve_reverse<<<nbk, B, 0, st>>>(rec, rec__, tag, N); count_launch(); }
-                { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec, basin_saddlenode, out, N, 0); count_launch(); }
-                PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :526
-            }
-        } else {
+        if (!carve) {
             { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec_, basin_saddlenode, out, N, 1); count_launch(); }  // :529
+            PFF_TRY(check_cuda("pff_reroute_flow"));
+            continue;
+        }
+        // ---- reroute_carve (:405-438) ----
+        PFF_CUDA(cudaMemsetAsync(tag, 0, (size_t)N, st));
+        PFF_CUDA(cudaMemsetAsync(tag_, 0, (size_t)N, st));
+        if (nonlocal) {
+            // general receivers: the reference's tag propagation by pointer jumping
+            { k_carve_tag_saddles<<<nbk, B, 0, st>>>(basin_saddlenode, tag, N); count_launch(); }
+            PFF_CUDA(cudaMemcpyAsync(tag_, tag, (size_t)N, cudaMemcpyDeviceToDevice, st));
+            PFF_CUDA(cudaMemcpyAsync(rec, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+            PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
+            int *cflags = w.ctr + 192;
+            PFF_CUDA(cudaMemsetAsync(cflags, 0, sizeof(int) * 64, st));
+            const int carve_rounds = ceil_log2(N) + 2;
+            for (int r = 0; r < carve_rounds; ++r) {
+                { k_carve_it1<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
+                { k_carve_it2<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
+            }
+            PFF_CUDA(cudaMemcpyAsync(rec, rec__, nb4, cudaMemcpyDeviceToDevice, st));
+            { k_carve_reverse<<<nbk, B, 0, st>>>(rec, rec__, tag, N); count_launch(); }
+            { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec, basin_saddlenode, out, N, 0); count_launch(); }
+            PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :526
+            PFF_TRY(check_cuda("pff_reroute_flow"));
+            continue;
+        }
+        // rec == rec_ here; rec__ holds the tile terminals of rec_
+        { k_carve_segments<<<grid, B, 0, st>>>(basin_saddlenode, rec_, rec, tag, tag_, rec__, w.pits[par], np, N, nx,
+                                               w.segs, w.ctr + 41, N, w.ctr + 43, w.dirty); count_launch(); }
+        { k_carve_walk<<<grid, B, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, w.dirty); count_launch(); }
+        { k_carve_link_list<<<grid, B, 0, st>>>(rec, basin_saddlenode, out, w.pits[par], np, N, w.dirty, nx); count_launch(); }
+        { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0); count_launch(); }  // :526
+        // ---- next iteration: pits left, labels by basin relabelling, dirty tiles ----
+        int *np_next = w.ctr + 16 * (par ^ 1);
+        PFF_CUDA(cudaMemsetAsync(np_next, 0, 4 * sizeof(int), st));
+        { k_relabel_init<<<grid, B, 0, st>>>(w.fin, bid, basin_saddlenode, out, w.pits[par], np, N, w.pits[par ^ 1],
+                                             np_next, w.ctr + 45); count_launch(); }
+        { k_dirty_list<<<div_up(ntiles, B), B, 0, st>>>(w.dirty, ntiles, w.tiles, w.ctr + 44); count_launch(); }
+        int h[3];
+        PFF_CUDA(cudaMemcpyAsync(h, w.ctr + 43, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        PFF_CUDA(cudaMemcpyAsync(&nd_next, np_next, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PFF_CUDA(cudaStreamSynchronize(st));
+        if (h[0]) break;  // walk bounds exceeded: reported below
+        const int ndirty = h[1];
+        // a reversed path without an outlet link (only for elevations >= 1e9): the
+        // pit bookkeeping below does not hold, relabel from scratch next iteration
+        const bool inc_ok = (h[2] == 0);
+        if (it + 1 >= outer) break;  // :500
+        if (inc_ok && nd_next == 0) {
+            ++n_outer;  // the next iteration would count 0 pits, label, then break (:512-514)
+            break;      // its labels are reset by basin_id_init (:537) anyway
+        }
+        incremental = inc_ok;
+        if (incremental) {
+            int *flags = w.ctr + 256;
+            PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
+            static int coop_relabel = 0;
+            if (!coop_relabel) {
+                int per = 0;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relabel_jump_coop, 256, 0);
+                coop_relabel = nsm * (per < 4 ? per : 4);
+            }
+            int *plist = w.pits[par];
+            void *args[] = {&w.fin, &plist, &np, &flags};
+            PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, st));
+            count_launch();
+            { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, N, ((uintptr_t)bid & 15) == 0); count_launch(); }
+            PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, ndirty, st);
         }
         PFF_TRY(check_cuda("pff_reroute_flow"));
     }

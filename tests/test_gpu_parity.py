@@ -139,7 +139,8 @@ def test_reroute(orc, cuda, mode, carve):
     torch = cuda
     from pyfastflow_b200 import flow
 
-    for kind, (nx, ny) in [("spectral", (211, 173)), ("int", (64, 48)), ("int", (9, 7)), ("uniform", (130, 66))]:
+    for kind, (nx, ny) in [("spectral", (211, 173)), ("int", (64, 48)), ("int", (9, 7)), ("uniform", (130, 66)),
+                           ("spectral", (512, 384))]:
         g = Grid(orc, torch, nx, ny, mode, seed=7)
         z = make_case(kind, nx, ny, seed=31 + mode)
         set_constants(g, 10.0)

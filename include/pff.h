@@ -131,6 +131,21 @@ int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_t *receiver
                          int32_t *receivers_, int32_t *receivers__, double epsilon, int N,
                          void *workspace, size_t workspace_bytes, void *stream);
 
+/* The same fill for callers that cannot allocate device memory (no workspace
+ * argument): its scratch is a 16 MiB device array built into the library,
+ * held on every GPU that loads the library until exit.  No counterpart in the
+ * reference.  Limits and rules:
+ *   - N <= PFF_NOALLOC_MAX_CELLS, else PFF_ERR_ARG;
+ *   - the first call on a device looks up that array's device address, so make
+ *     the first call on each device before any stream capture;
+ *   - calls share the one array: calls that overlap on the GPU (other streams,
+ *     other host threads) race and must be serialised by the caller.
+ * Never calls cudaMalloc/cudaFree.  Same results as pff_fill_z_add_delta. */
+#define PFF_NOALLOC_MAX_CELLS (1 << 22)
+int pff_fill_z_add_delta_noalloc(float *zh, float *h, float *z_, const int32_t *receivers,
+                                 int32_t *receivers_, int32_t *receivers__, double epsilon, int N,
+                                 void *stream);
+
 /* graphflood/gf_hydrodynamics.py:24-75 diffuse_Q_constant_prec(zh, Q, temp), run
  * `nsweeps` times (the Flooder runs 5).  prec_dx2 = float(PREC*DX*DX).  Sums are
  * formed in the reference's serial order (ascending source cell, then k), so the

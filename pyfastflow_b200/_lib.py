@@ -35,6 +35,7 @@ SIGNATURES = {
     "pff_saddlesort": (_i32, [_vp] * 7 + [_i32, _i32, _i32, _vp, _vp]),
     "pff_fill_workspace_bytes": (_sz, [_i32]),
     "pff_fill_z_add_delta": (_i32, [_vp] * 6 + [_f64, _i32, _vp, _sz, _vp]),
+    "pff_fill_z_add_delta_noalloc": (_i32, [_vp] * 6 + [_f64, _i32, _vp]),
     "pff_diffuse_workspace_bytes": (_sz, [_i32]),
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),

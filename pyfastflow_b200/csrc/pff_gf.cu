@@ -194,6 +194,75 @@ extern "C" int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_
     return check_cuda("pff_fill_z_add_delta");
 }
 
+// ---- fill without caller-provided scratch -----------------------------------------
+//
+// For callers that cannot allocate device memory (for example code running
+// under an allocator that forbids new allocations, or a host that only hands
+// out the buffers it owns): the one scratch buffer of the fill -- the
+// start-of-round snapshot of z_ -- lives in this file-scope device array
+// instead of a workspace.  It holds PFF_NOALLOC_MAX_CELLS floats (16 MiB) on
+// every GPU that loads the library, until the process exits.
+static __device__ __align__(256) float g_fill_scratch[PFF_NOALLOC_MAX_CELLS];
+
+// Device address of g_fill_scratch per device, looked up once with that device
+// current (the host-side symbol is only a stand-in, not a device address).
+static float *g_fill_scratch_ptr[64] = {nullptr};
+
+static int fill_scratch_address(float **out)
+{
+    int dev = 0;
+    PFF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("pff_fill_z_add_delta_noalloc: device index %d out of range", dev);
+        return PFF_ERR_ARG;
+    }
+    if (!g_fill_scratch_ptr[dev]) {
+        void *p = nullptr;
+        PFF_CUDA(cudaGetSymbolAddress(&p, g_fill_scratch));
+        g_fill_scratch_ptr[dev] = (float *)p;
+    }
+    *out = g_fill_scratch_ptr[dev];
+    return PFF_OK;
+}
+
+extern "C" int pff_fill_z_add_delta_noalloc(float *zh, float *h, float *z_, const int32_t *receivers,
+                                            int32_t *receivers_, int32_t *receivers__, double epsilon, int N,
+                                            void *stream)
+{
+    clear_error();
+    if (N <= 1 || !zh || !h || !z_ || !receivers || !receivers_ || !receivers__) {
+        set_error("pff_fill_z_add_delta_noalloc: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    if (N > PFF_NOALLOC_MAX_CELLS) {
+        set_error("pff_fill_z_add_delta_noalloc: %d cells exceed the built-in scratch of %d cells; "
+                  "use pff_fill_z_add_delta with a workspace",
+                  N, PFF_NOALLOC_MAX_CELLS);
+        return PFF_ERR_ARG;
+    }
+    float *zt = nullptr;
+    PFF_TRY(fill_scratch_address(&zt));
+    cudaStream_t st = S(stream);
+    const size_t nbf = sizeof(float) * (size_t)N, nbi = sizeof(int32_t) * (size_t)N;
+    PFF_CUDA(cudaMemcpyAsync(z_, zh, nbf, cudaMemcpyDeviceToDevice, st));
+    PFF_CUDA(cudaMemcpyAsync(receivers_, receivers, nbi, cudaMemcpyDeviceToDevice, st));
+    int nr = 0;
+    for (long long p = 1; p < N; p <<= 1) ++nr;
+    // every round writes all N snapshot entries before any is read: nothing to clear
+    float *zs = z_, *zn = zt;
+    int32_t *ra = receivers_, *rb = receivers__;
+    for (int it = 0; it < nr; ++it) {
+        const float inc = (float)(ldexp(1.0, it - 1) * epsilon);
+        { k_fill_round<<<div_up(N, 256), 256, 0, st>>>(zh, zs, zn, ra, rb, inc, N); count_launch(); }
+        float *tz = zs; zs = zn; zn = tz;
+        int32_t *tr = ra; ra = rb; rb = tr;
+    }
+    if (zs != z_) PFF_CUDA(cudaMemcpyAsync(z_, zs, nbf, cudaMemcpyDeviceToDevice, st));
+    PFF_CUDA(cudaMemcpyAsync(rb, ra, nbi, cudaMemcpyDeviceToDevice, st));
+    { k_fill_apply<<<div_up(N, 256), 256, 0, st>>>(zh, h, z_, N); count_launch(); }
+    return check_cuda("pff_fill_z_add_delta_noalloc");
+}
+
 extern "C" size_t pff_diffuse_workspace_bytes(int N)
 {
     return Carver::round(sizeof(float4) * (size_t)N) + Carver::round((size_t)N) + 512;

@@ -50,47 +50,94 @@ int check_grid(int nx, int ny, int mode, const uint8_t *codes)
 
 // ---------------------------------------------------------------------------
 // Receivers: pyfastflow/flow/receivers.py:31-58.
-// One thread per cell of a 2-D block; the four neighbour loads of a block hit
-// L1/L2 (each z row is read from DRAM once per block row band).
-template <int MODE>
-__global__ void __launch_bounds__(256) k_receivers(const float *__restrict__ z, int32_t *__restrict__ rcv,
-                                                   float *__restrict__ grad, Grid g, float dx)
+//
+// Each warp walks a 32-column strip down RCV_ROWS rows: the cell's own row and
+// the rows above and below stay in registers (one coalesced 128-byte load per
+// row), left and right neighbours come from the adjacent lanes by shuffle (the
+// two strip-edge lanes load one extra value).  Cells on the grid edge, and the
+// custom mode, use the generic neighbour rules with direct loads.
+
+// D4 receiver of cell i from its own and its neighbours' elevations.  A drop can
+// only beat the best so far if it exceeds the best drop so far (division by
+// dx > 0 is monotone), so the IEEE division -- the costly part -- runs only for
+// improving candidates; the comparison is still between rounded quotients, as in
+// the reference (strict '>', ties after rounding keep the earlier k).
+__device__ __forceinline__ void rcv_pick(float zi, const float (&zn)[4], const int (&jn)[4], float dx, int &r,
+                                         float &sr)
 {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = blockIdx.y * blockDim.y + threadIdx.y;
-    if (col >= g.nx || row >= g.ny) return;
-    const int i = row * g.nx + col;
-    const float zi = z[i];
-    int r = i;
-    float sr = 0.f;
-    // A drop d can only beat the current best if d exceeds the best drop so far
-    // (division by dx > 0 is monotone), so the IEEE division -- the costly part --
-    // runs only for improving candidates; the comparison is still on the rounded
-    // quotients, as in the reference (ties after rounding keep the earlier k).
     float dbest = 0.f;
-    int js[4];
-    neighbours4<MODE>(g, i, row, col, js);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const int j = js[k];
-        if (j != -1) {
-            const float d = __fsub_rn(zi, __ldg(z + j));
-            if (d > dbest) {
-                const float tsr = __fdiv_rn(d, dx);
-                if (tsr > sr) { sr = tsr; r = j; dbest = d; }
-            }
+        if (jn[k] == -1) continue;
+        const float d = __fsub_rn(zi, zn[k]);
+        if (d > dbest) {
+            const float tsr = __fdiv_rn(d, dx);
+            if (tsr > sr) { sr = tsr; r = jn[k]; dbest = d; }
         }
     }
-    rcv[i] = r;
-    grad[i] = sr;
+}
+
+constexpr int RCV_ROWS = 32;
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, int32_t *__restrict__ rcv,
+                                                   float *__restrict__ grad, Grid g, float dx)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nstrips = (g.nx + 31) >> 5;
+    const int strip = warp % nstrips, band = warp / nstrips;
+    const int col = (strip << 5) + lane;
+    const int row0 = band * RCV_ROWS;
+    if (row0 >= g.ny) return;
+    const int row1 = min(row0 + RCV_ROWS, g.ny);
+    const bool incol = col < g.nx;
+    const int nx = g.nx;
+    // register window: above, centre, below (column `col`)
+    float za = 0.f, zc = 0.f, zb = 0.f;
+    if (incol) {
+        zc = __ldg(z + (size_t)row0 * nx + col);
+        if (row0 > 0) za = __ldg(z + (size_t)(row0 - 1) * nx + col);
+    }
+    for (int row = row0; row < row1; ++row) {
+        const int i = row * nx + col;
+        if (incol && row + 1 < g.ny) zb = __ldg(z + (size_t)(row + 1) * nx + col);
+        // left/right from the neighbouring lanes; strip-edge lanes load their own
+        float zl = __shfl_up_sync(0xffffffffu, zc, 1);
+        float zr = __shfl_down_sync(0xffffffffu, zc, 1);
+        if (incol) {
+            if (lane == 0 && col > 0) zl = __ldg(z + i - 1);
+            if ((lane == 31 || col == nx - 1) && col + 1 < nx) zr = __ldg(z + i + 1);
+            int r = i;
+            float sr = 0.f;
+            if (MODE != 3 && row > 0 && row < g.ny - 1 && col > 0 && col < nx - 1) {
+                const float zn[4] = {za, zl, zr, zb};
+                const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                rcv_pick(zc, zn, jn, dx, r, sr);
+            } else {
+                int jn[4];
+                float zn[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    jn[k] = neighbour<MODE>(g, i, row, col, k);
+                    zn[k] = jn[k] != -1 ? __ldg(z + jn[k]) : 0.f;
+                }
+                rcv_pick(zc, zn, jn, dx, r, sr);
+            }
+            rcv[i] = r;
+            grad[i] = sr;
+        }
+        za = zc;
+        zc = zb;
+    }
 }
 
 template <int MODE>
 static void launch_receivers(const float *z, int32_t *rcv, float *grad, const Grid &g, float dx,
                              cudaStream_t st)
 {
-    dim3 b(32, 8), gr(div_up(g.nx, 32), div_up(g.ny, 8));
-    { k_receivers<MODE><<<gr, b, 0, st>>>(z, rcv, grad, g, dx); count_launch(); }
+    const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + RCV_ROWS - 1) / RCV_ROWS);
+    { k_receivers<MODE><<<div_up(warps, 4), 128, 0, st>>>(z, rcv, grad, g, dx); count_launch(); }
 }
 
 }  // namespace pff

@@ -492,6 +492,105 @@ __global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restri
     block_append<256>(border && bid[i] != 0, i, blist, nblist);
 }
 
+// Pass 1+2 as a column-strip stencil: each warp walks a 32-column strip down
+// SAD_ROWS rows with bid and z of the rows above/at/below in registers and the
+// left/right values from neighbouring lanes.  Border cells of pit basins collect
+// in a per-warp shared buffer, flushed with one atomic per strip.
+constexpr int SAD_ROWS = 32;
+
+template <int MODE>
+__device__ __forceinline__ bool saddle_cell(int i, int row, int col, const Grid &g, int bi, float zi, const int (&jn)[4],
+                                            const int (&bn)[4], const float (&zn)[4], uint8_t *is_border, float *zp,
+                                            long long *saddle)
+{
+    bool border = false;
+    float zmin = 1e9f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (jn[k] != -1 && bn[k] != bi) { border = true; zmin = fminf(zmin, zn[k]); }
+    is_border[i] = border;
+    const float zpi = border ? fmaxf(zi, zmin) : 1e9f;
+    zp[i] = zpi;
+    if (!border) return false;
+    const long long iv = invalid_key();
+    long long res = iv;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (jn[k] == -1 || bn[k] == bi) continue;
+        const long long c = pack_key(zpi, bn[k]);
+        res = c < res ? c : res;
+    }
+    if (res != iv) atomicMin(saddle + bi, res);
+    return bi != 0;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restrict__ bid, uint8_t *is_border,
+                                                          float *zp, long long *saddle, const float *__restrict__ z,
+                                                          Grid g, int *blist, int *nblist)
+{
+    __shared__ int buf[4][32 * SAD_ROWS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int warp = blockIdx.x * 4 + wib;
+    const int nx = g.nx, ny = g.ny;
+    const int nstrips = (nx + 31) >> 5;
+    const int strip = warp % nstrips, band = warp / nstrips;
+    const int col = (strip << 5) + lane;
+    const int row0 = band * SAD_ROWS;
+    if (row0 >= ny) return;
+    const int row1 = min(row0 + SAD_ROWS, ny);
+    const bool incol = col < nx;
+    int nb = 0;  // border cells buffered by this warp
+    int ba = 0, bc = 0, bb = 0;
+    float za = 0.f, zc = 0.f, zb = 0.f;
+    if (incol) {
+        bc = bid[row0 * nx + col];
+        zc = z[row0 * nx + col];
+        if (row0 > 0) { ba = bid[(row0 - 1) * nx + col]; za = z[(row0 - 1) * nx + col]; }
+    }
+    for (int row = row0; row < row1; ++row) {
+        const int i = row * nx + col;
+        if (incol && row + 1 < ny) { bb = bid[i + nx]; zb = z[i + nx]; }
+        int bl = __shfl_up_sync(0xffffffffu, bc, 1), br = __shfl_down_sync(0xffffffffu, bc, 1);
+        float zl = __shfl_up_sync(0xffffffffu, zc, 1), zr = __shfl_down_sync(0xffffffffu, zc, 1);
+        bool listed = false;
+        if (incol) {
+            const bool interior = MODE != 3 && row > 0 && row < ny - 1 && col > 0 && col < nx - 1;
+            if (interior) {
+                if (lane == 0) { bl = bid[i - 1]; zl = z[i - 1]; }
+                if (lane == 31) { br = bid[i + 1]; zr = z[i + 1]; }
+                // interior cells of modes 0-2 never leave the domain
+                const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                const int bn[4] = {ba, bl, br, bb};
+                const float zn[4] = {za, zl, zr, zb};
+                listed = saddle_cell<MODE>(i, row, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+            } else if (can_leave<MODE>(g, i, row, col)) {
+                zp[i] = zc;
+            } else {
+                int jn[4], bn[4];
+                float zn[4];
+                neighbours4<MODE>(g, i, row, col, jn);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    bn[k] = jn[k] != -1 ? bid[jn[k]] : 0;
+                    zn[k] = jn[k] != -1 ? z[jn[k]] : 0.f;
+                }
+                listed = saddle_cell<MODE>(i, row, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, listed);
+        if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = i;
+        nb += __popc(m);
+        ba = bc; bc = bb;
+        za = zc; zc = zb;
+    }
+    __syncwarp();
+    int base = 0;
+    if (lane == 0 && nb) base = atomicAdd(nblist, nb);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (int k = lane; k < nb; k += 32) blist[base + k] = buf[wib][k];
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_saddle_p3_list(const int32_t *__restrict__ bid, const float *__restrict__ zp,
                                                         const long long *__restrict__ saddle, int32_t *snode, Grid g,
@@ -829,8 +928,8 @@ static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long lon
                            const int *np, int *blist, int *nblist, int grid, cudaStream_t st)
 {
     const int N = g.N();
-    dim3 gr(div_up(g.nx, 32), div_up(g.ny, 8));
-    { k_saddle_p12_list<MODE><<<gr, 256, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist); count_launch(); }
+    const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + SAD_ROWS - 1) / SAD_ROWS);
+    { k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist); count_launch(); }
     { k_saddle_p3_list<MODE><<<grid, 256, 0, st>>>(bid, zp, saddle, snode, g, blist, nblist); count_launch(); }
     { k_saddle_p4_list<MODE><<<grid, 256, 0, st>>>(bid, saddle, snode, outlet, z, g, pits, np); count_launch(); }
     { k_saddle_p5_decide_list<<<grid, 256, 0, st>>>(bid, outlet, inv, N, pits, np); count_launch(); }

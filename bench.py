@@ -138,7 +138,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="routing", choices=["routing", "graphflood"])
+    ap.add_argument("--max-iter", type=int, default=20000)
+    ap.add_argument("--fp64-size", type=int, default=256)
+    ap.add_argument("--fp64-iters", type=int, default=200)
     args = ap.parse_args()
+    if args.workload == "graphflood":
+        return graphflood_main(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -290,6 +296,104 @@ def main():
         print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+GF_METRIC = "graphflood s-to-residual"
+
+
+def graphflood_main(args):
+    """GraphFlood on the 2048 x 2048 DEM (dx 10 m, P 1e-5 m/s, n 0.033, h0 = 0,
+    DT_HYDRO 5e-3): seconds until max|dh|/dt < 1e-4 * P or --max-iter iterations."""
+    import torch
+
+    import pyfastflow_b200 as pf
+    from pyfastflow_b200 import _lib, synthetic
+
+    n = args.size if args.size != 4096 else 2048
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    w = synthetic.graphflood_plain(n)
+    z = w["z"]
+    P = 1e-5
+    router = pf.flow.FlowRouter(n, n, 10.0)
+    fl = pf.graphflood.Flooder(router, precipitation_rates=P, manning=0.033, edge_slope=1e-2)
+
+    def reset():
+        router.set_z(z)
+        router.Q.zero_()
+        fl.h.zero_()
+
+    reset()
+    for _ in range(args.warmup):
+        fl.iteration()
+    torch.cuda.synchronize()
+    reset()
+    torch.cuda.synchronize()
+    l0 = lib.pff_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        e0.record()
+        iters, reason, res, trace = fl.run_to_residual(tol_ratio=1e-4, max_iter=args.max_iter, return_trace=True)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    dev_s = e0.elapsed_time(e1) / 1e3
+    launches = (lib.pff_launch_count() - l0) / max(iters, 1)
+    h = fl.get_h()
+    tr = [float(x) for x in trace]
+    out = {"metric": GF_METRIC, "value": dev_s, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": args.warmup,
+           "ms_per_step": dev_s * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic (seeded spectral DEM + Gaussian pits)",
+           "config": {"workload": f"graphflood_plain {n}x{n}, dx 10 m, P 1e-5 m/s, n 0.033, h0 0, dt 5e-3, "
+                                  "stop max|dh|/dt < 1e-4 P or max_iter", "max_iter": args.max_iter},
+           "iterations": iters, "stop": reason, "final_residual": res,
+           "ms_per_iteration": dev_s * 1e3 / max(iters, 1), "wall_s": wall, "gpu_launches_per_iteration": launches,
+           "residual_trace": {str(k): tr[k - 1] for k in (1, 10, 100, 1000, 5000, 10000, 20000) if k <= len(tr)},
+           "h_stats": {"max": float(np.nanmax(h)), "mean": float(np.nanmean(h)), "nan": int(np.isnan(h).sum()),
+                       "wet_cells_1cm": int((h > 0.01).sum())},
+           "clocks": clk.summary()}
+    if args.fp64_iters > 0:
+        out["fp64_check"] = graphflood_fp64_check(args.fp64_size, args.fp64_iters)
+    print(json.dumps(out))
+
+
+def graphflood_fp64_check(n, iters):
+    """The same GraphFlood update run on an n x n DEM of the same generator for
+    `iters` iterations: GPU f32 vs the CPU restatement in f32 (must match bit for
+    bit) and in f64 (error reported)."""
+    import torch
+
+    import pyfastflow_b200 as pf
+    from oracle import oracle as O
+    from pyfastflow_b200 import synthetic
+
+    O.build()
+    z = synthetic.graphflood_plain(n)["z"]
+    P = 1e-5
+    router = pf.flow.FlowRouter(n, n, 10.0)
+    router.set_z(z)
+    fl = pf.graphflood.Flooder(router, precipitation_rates=P, manning=0.033, edge_slope=1e-2)
+    fl.run_graphflood(iters)
+    torch.cuda.synchronize()
+    h32, Q32 = fl.get_h().ravel().astype(np.float64), router.get_Q().ravel().astype(np.float64)
+    g = O.Grid(n, n, 0)
+    zo, ho, Qo = z.ravel().copy(), np.zeros(n * n, np.float32), np.zeros(n * n, np.float32)
+    O.graphflood_run(zo, ho, Qo, g, 10.0, P, niter=iters)
+    z6, h6, Q6 = z.ravel().astype(np.float64), np.zeros(n * n), np.zeros(n * n)
+    O.graphflood_run(z6, h6, Q6, g, 10.0, P, niter=iters, f64=True)
+    wet = h6 > 1e-3
+    rel_h = np.abs(h32 - h6)[wet] / h6[wet]
+    rel_q = np.abs(Q32 - Q6) / np.maximum(np.abs(Q6), 1e-30)
+    return {"grid": f"{n}x{n}", "iterations": iters,
+            "gpu_vs_cpu_f32_bit_exact": bool(np.array_equal(fl.get_h().ravel().view(np.uint32), ho.view(np.uint32))
+                                             and np.array_equal(router.get_Q().ravel().view(np.uint32),
+                                                                Qo.view(np.uint32))),
+            "h_abs_err_vs_f64": {"max": float(np.abs(h32 - h6).max()), "mean": float(np.abs(h32 - h6).mean())},
+            "h_rel_err_vs_f64_wet": {"max": float(rel_h.max()) if rel_h.size else None,
+                                     "mean": float(rel_h.mean()) if rel_h.size else None,
+                                     "wet_cells_over_1mm": int(wet.sum())},
+            "Q_rel_err_vs_f64": {"max": float(rel_q.max()), "mean": float(rel_q.mean())}}
 
 
 if __name__ == "__main__":

@@ -10,6 +10,7 @@
 //     decisions plus the one basin whose serial outcome can differ
 //     (k_saddle_p5_serial_fix).
 #include <cooperative_groups.h>
+#include <cstdlib>
 #include <cub/block/block_scan.cuh>
 #include "pff_internal.h"
 #include "pff_tiles.cuh"
@@ -418,11 +419,13 @@ __global__ void __launch_bounds__(256) k_border_jump_coop(int32_t *R, int nx, in
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_labels_final(const int32_t *__restrict__ J, const int32_t *__restrict__ R,
-                                                      int32_t *bid, Grid g)
+                                                      int32_t *bid, Grid g, const int32_t *__restrict__ rec,
+                                                      int *unresolved)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.N()) return;
     const int root = r_get(R, g.nx, g.ny, J[i]);
+    if (rec[root] != root) *unresolved = 1;  // a receiver cycle: labels need the general path
     bid[i] = can_leave_i<MODE>(g, root) ? 0 : root + 1;
 }
 
@@ -876,6 +879,130 @@ __global__ void __launch_bounds__(256) k_sync_tagged(int32_t *rec_, const int32_
     }
 }
 
+// ---- receiver cycles: the reference's serial semantics ------------------------------
+//
+// A carve can close a cycle of basins (b -> b' -> b'' -> b with tied saddles;
+// the 2-cycle pass removes only length 2), and then the receivers hold a cycle.
+// The reference resolves it in its next outer iteration through two serial
+// effects, reproduced here exactly:
+//   - labels: serial in-place pointer jumping (lakeflow.py:64-80) on a cycle
+//     depends only on the cycle's cells, visited in ascending index; it is
+//     emulated per cycle (k_cycle_emulate), every other cell takes the fixed point;
+//   - reversal: several tagged cells can share a tagged receiver; the serial
+//     last writer is the largest index (k_rev_claim / k_rev_apply).
+
+// unresolved cell: its jumped pointer did not reach a true root
+__global__ void k_cycle_find(const int32_t *__restrict__ rec, const int32_t *__restrict__ work, int N, int *entries,
+                             int *nentries, int cap, int32_t *mark)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int r = work[i];
+    if (rec[r] == r) return;
+    if (atomicExch(mark + r, 1) == 0) {
+        const int slot = atomicAdd(nentries, 1);
+        if (slot < cap) entries[slot] = r;
+    }
+}
+
+constexpr int CYC_MAX = 4096;
+
+// One thread: walk each cycle reached by the entries, emulate the serial rounds
+// on it, record the resulting label of every cycle cell in cyc_label.
+template <int MODE>
+__global__ void k_cycle_emulate(const int32_t *__restrict__ rec, const int *__restrict__ entries, const int *nentries,
+                                int cap, int32_t *cyc_label, int32_t *done, Grid g, int rounds, int *err)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ int cells[CYC_MAX];
+    __shared__ int lrec[CYC_MAX];
+    __shared__ int lbid[CYC_MAX];
+    const int n = min(*nentries, cap);
+    for (int e = 0; e < n; ++e) {
+        int x = entries[e];
+        // move onto the cycle: from any cell of a cyclic component, N steps land on it
+        for (int s = 0; s < CYC_MAX && !done[x]; ++s) x = rec[x];
+        if (done[x]) continue;
+        // a cell reached after CYC_MAX steps lies on the cycle if the cycle is shorter
+        int L = 0, y = x;
+        do {
+            if (L >= CYC_MAX) { *err = 1; break; }
+            cells[L++] = y;
+            y = rec[y];
+        } while (y != x);
+        if (y != x) continue;
+        // ascending index order, as the serial loop visits them
+        for (int a = 1; a < L; ++a) {
+            int v = cells[a], b = a - 1;
+            while (b >= 0 && cells[b] > v) { cells[b + 1] = cells[b]; --b; }
+            cells[b + 1] = v;
+        }
+        for (int a = 0; a < L; ++a) {
+            const int c = cells[a];
+            int lo = 0, hi = L - 1, t = rec[c];
+            while (lo < hi) { const int mid = (lo + hi) >> 1; if (cells[mid] < t) lo = mid + 1; else hi = mid; }
+            lrec[a] = lo;
+            lbid[a] = can_leave_i<MODE>(g, c) ? 0 : c + 1;
+        }
+        for (int r = 0; r < rounds; ++r)
+            for (int a = 0; a < L; ++a) {
+                lbid[a] = lbid[lrec[a]];
+                lrec[a] = lrec[lrec[a]];
+            }
+        for (int a = 0; a < L; ++a) {
+            cyc_label[cells[a]] = lbid[a];
+            done[cells[a]] = 1;
+            if (lbid[a] != lbid[0]) *err = 2;  // feeders' labels would depend on timing
+        }
+    }
+}
+
+// Unresolved cells take the label of the cycle cell their pointer ends on; all
+// cells of an emulated cycle end with one label (its in-place jumping converges
+// to a single self-loop), so the feeders' serial result is that label.
+__global__ void k_cycle_apply(const int32_t *__restrict__ rec, const int32_t *__restrict__ work,
+                              const int32_t *__restrict__ cyc_label, const int32_t *__restrict__ done, int32_t *bid, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int r = work[i];
+    if (rec[r] == r) return;
+    for (int s = 0; s < CYC_MAX && !done[r]; ++s) r = rec[r];
+    if (done[r]) bid[i] = cyc_label[r];
+}
+
+// finalise_reroute_carve's reversal (:395-397) with the serial last writer: the
+// largest tagged index claims each tagged receiver.
+__global__ void k_rev_claim(const int32_t *__restrict__ rec0, const uint8_t *__restrict__ tag, int32_t *claim, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int r = rec0[i];
+    if (tag[r] && tag[i] && i != r) atomicMax(claim + r, i);
+}
+__global__ void k_rev_apply(int32_t *rec, const int32_t *__restrict__ claim, int N)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= N) return;
+    const int c = claim[r];
+    if (c >= 0) rec[r] = c;
+}
+
+// Incremental relabel sanity.  Every acyclic chain ends at a basin that was not
+// carved (no valid outlet) or at 0; a chain that ends at a carved basin came
+// from a cycle (in-place jumping can collapse a cycle onto a fake fixed point, so
+// convergence alone proves nothing).
+__global__ void k_relabel_check(const int32_t *__restrict__ fin, const long long *__restrict__ outlet,
+                                const int *__restrict__ pits, const int *np, int N, int *flag)
+{
+    const int n = *np;
+    const long long iv = invalid_key();
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int f = fin[pits[k] + 1];
+        if (f != 0 && (f >= N || fin[f] != f || outlet[f] != iv)) *flag = 1;
+    }
+}
+
 // ---- launchers ---------------------------------------------------------------
 
 template <int MODE>
@@ -918,9 +1045,16 @@ static void l_tile_terminal_list(const int32_t *rec, int32_t *J, int32_t *R, int
     { k_tile_terminal<MODE><<<ntiles, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles); count_launch(); }
 }
 template <int MODE>
-static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, cudaStream_t st)
+static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, const int32_t *rec,
+                           int *unresolved, cudaStream_t st)
 {
-    { k_labels_final<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(J, R, bid, g); count_launch(); }
+    { k_labels_final<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(J, R, bid, g, rec, unresolved); count_launch(); }
+}
+template <int MODE>
+static void l_cycle_emulate(const int32_t *rec, const int *entries, const int *n, int cap, int32_t *lab, int32_t *done,
+                            const Grid &g, int rounds, int *err, cudaStream_t st)
+{
+    { k_cycle_emulate<MODE><<<1, 32, 0, st>>>(rec, entries, n, cap, lab, done, g, rounds, err); count_launch(); }
 }
 template <int MODE>
 static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long long *saddle, int32_t *snode,
@@ -1082,10 +1216,9 @@ static int tile_pass(const int32_t *rec, int32_t *Jbuf, const Grid &g, RerouteWs
 
 // Basin labels from a tile pass: pointer jumping over border cells, then one
 // gather per cell.
-static int tile_resolve(const int32_t *Jbuf, int32_t *bid, const Grid &g, RerouteWs &w, int parity, int grid,
-                        cudaStream_t st)
+static int tile_resolve(const int32_t *Jbuf, int32_t *bid, const Grid &g, RerouteWs &w, const int32_t *rec,
+                        int *unresolved, cudaStream_t st)
 {
-    (void)parity;
     int *flags = w.ctr + 64;
     PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
     static int coop_blocks = 0;
@@ -1102,9 +1235,29 @@ static int tile_resolve(const int32_t *Jbuf, int32_t *bid, const Grid &g, Rerout
     void *args[] = {&R, &nx, &ny, &ntx, &nslots, &flags};
     PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_border_jump_coop, coop_blocks, 256, args, 0, st));
     count_launch();
-    (void)grid;
-    PFF_MODE_DISPATCH(g.mode, l_labels_final, Jbuf, w.R, bid, g, st);
+    PFF_MODE_DISPATCH(g.mode, l_labels_final, Jbuf, w.R, bid, g, rec, unresolved, st);
     return check_cuda("tile_resolve");
+}
+
+// Labels of any receivers, with the reference's serial result on receiver
+// cycles: basin_id_init, pointer-jumping rounds on work = copy of rec, then the
+// cycle emulation for cells whose pointer did not reach a true root.
+static int general_labels(const int32_t *rec, int32_t *work, int32_t *bid, const Grid &g, RerouteWs &w, int *err,
+                          cudaStream_t st)
+{
+    const int N = g.N();
+    PFF_TRY(launch_basin_init(bid, g, st));
+    PFF_CUDA(cudaMemcpyAsync(work, rec, sizeof(int32_t) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    PFF_TRY(run_labels(bid, work, g, w.ctr + 128, st));
+    int *nentries = w.ctr + 46;
+    PFF_CUDA(cudaMemsetAsync(nentries, 0, sizeof(int), st));
+    PFF_CUDA(cudaMemsetAsync(w.segs, 0, sizeof(int) * (size_t)N, st));   // mark
+    PFF_CUDA(cudaMemsetAsync(w.blist, 0, sizeof(int) * (size_t)N, st));  // done
+    { k_cycle_find<<<div_up(N, 256), 256, 0, st>>>(rec, work, N, w.tiles, nentries, N, w.segs); count_launch(); }
+    PFF_MODE_DISPATCH(g.mode, l_cycle_emulate, rec, w.tiles, nentries, N, w.fin, w.blist, g, ceil_log2(N) + 1, err,
+                      st);
+    { k_cycle_apply<<<div_up(N, 256), 256, 0, st>>>(rec, work, w.fin, w.blist, bid, N); count_launch(); }
+    return check_cuda("general_labels");
 }
 
 }  // namespace pff
@@ -1144,56 +1297,68 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
     const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(ny, TILE_H);
     PFF_CUDA(cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, st));
     int outer = 0, n_outer = 0;
-    // In carve mode with D4 receivers, labels after iteration 0 come from relabelling
-    // basin ids (k_relabel_*), and tile terminals are recomputed for dirty tiles only.
+    // Fast mode (carve, D4 receivers, no receiver cycle): tile labels in the first
+    // iteration, basin relabelling and dirty-tile terminals afterwards, list-driven
+    // saddle passes, tile-walk carving.  General mode (jump rerouting, non-D4
+    // receivers, or once a receiver cycle appears): the reference's own steps with
+    // its serial semantics, N-wide.
+    bool general = !carve;
     bool incremental = false;
     int nd_next = 0;
+    int *cyc_err = w.ctr + 47;
+    static const bool trace = getenv("PFF_TRACE_REROUTE") != nullptr;  // diagnostic trace on stderr
     for (int it = 0;; ++it) {
         if (it > 0 && it >= outer) break;  // :500
         const int par = it & 1;
         int *np = w.ctr + 16 * par;
-        int nd_bis = 0, nonlocal = 1;
-        if (incremental) {
+        int nd_bis = 0;
+        if (incremental && !general) {
             nd_bis = nd_next;  // pits left after the previous carve; bid already relabelled
-            nonlocal = 0;
+        } else if (!general && it == 0) {
+            int nonlocal = 0;
+            PFF_TRY(tile_pass(rec_, rec__, g, w, par, &nd_bis, &nonlocal, st));  // :493, :501
+            if (nonlocal) general = true;
         } else {
-            // depression_counter(rec_) (:493, :501), with the pit list
-            if (carve) {
-                PFF_TRY(tile_pass(rec_, rec__, g, w, par, &nd_bis, &nonlocal, st));
-            } else {
-                PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
-                PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);
-                PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
-                PFF_CUDA(cudaStreamSynchronize(st));
-            }
+            PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
+            PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);  // :501
+            PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PFF_CUDA(cudaStreamSynchronize(st));
         }
         if (it == 0) {
             if (nd_bis == 0) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
             outer = ceil_log2(nd_bis) + 1;                            // :500
         }
-        if (!incremental) {
-            // basin labels: basin_id_init + propagate_basin on rec__ = rec_ (:507-511)
-            if (!nonlocal) {
-                PFF_TRY(tile_resolve(rec__, bid, g, w, par, grid, st));
-            } else {
-                PFF_TRY(launch_basin_init(bid, g, st));
-                PFF_CUDA(cudaMemcpyAsync(rec__, rec_, nb4, cudaMemcpyDeviceToDevice, st));
-                PFF_TRY(run_labels(bid, rec__, g, w.ctr + 128, st));
-            }
+        // basin labels: basin_id_init + propagate_basin on rec__ = rec_ (:507-511)
+        if (!general && !incremental) {
+            int *unres = w.ctr + 48;
+            PFF_CUDA(cudaMemsetAsync(unres, 0, sizeof(int), st));
+            PFF_TRY(tile_resolve(rec__, bid, g, w, rec_, unres, st));
+            int u = 0;
+            PFF_CUDA(cudaMemcpyAsync(&u, unres, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PFF_CUDA(cudaStreamSynchronize(st));
+            if (u) general = true;  // the input receivers hold a cycle
         }
+        if (general) PFF_TRY(general_labels(rec_, rec__, bid, g, w, cyc_err, st));
+        if (trace) fprintf(stderr, "[pff reroute] it %d outer %d pits %d general %d incremental %d\n", it, outer, nd_bis,
+                           (int)general, (int)incremental);
         ++n_outer;
         if (nd_bis == 0) break;  // :512-514
-        // ---- saddlesort (:520), list driven ----
-        if (it == 0) {
-            { k_basin_arrays_init<<<div_up(N + 1, B), B, 0, st>>>(sad, out, basin_saddlenode, w.inv, N + 1); count_launch(); }
+        // ---- saddlesort (:520) ----
+        if (general) {
+            // every basin id, as the reference loops (cycle basins are not pits)
+            PFF_MODE_DISPATCH(bound_mode, l_saddle, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z, g, st);
         } else {
-            // the previous saddlesort wrote only the entries of its pits (a superset of the current ones) and 0
-            { k_basin_reset_list<<<grid, B, 0, st>>>(sad, out, basin_saddlenode, w.inv, w.pits[par ^ 1],
-                                                     w.ctr + 16 * (par ^ 1)); count_launch(); }
+            if (it == 0) {
+                { k_basin_arrays_init<<<div_up(N + 1, B), B, 0, st>>>(sad, out, basin_saddlenode, w.inv, N + 1); count_launch(); }
+            } else {
+                // the previous saddlesort wrote only the entries of its pits (a superset of the current ones) and 0
+                { k_basin_reset_list<<<grid, B, 0, st>>>(sad, out, basin_saddlenode, w.inv, w.pits[par ^ 1],
+                                                         w.ctr + 16 * (par ^ 1)); count_launch(); }
+            }
+            PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 6 * sizeof(int), st));
+            PFF_MODE_DISPATCH(bound_mode, l_saddle_lists, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z,
+                              g, w.pits[par], np, w.blist, w.ctr + 40, grid, st);
         }
-        PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 6 * sizeof(int), st));
-        PFF_MODE_DISPATCH(bound_mode, l_saddle_lists, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z, g,
-                          w.pits[par], np, w.blist, w.ctr + 40, grid, st);
         if (!carve) {
             { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec_, basin_saddlenode, out, N, 1); count_launch(); }  // :529
             PFF_TRY(check_cuda("pff_reroute_flow"));
@@ -1202,8 +1367,8 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         // ---- reroute_carve (:405-438) ----
         PFF_CUDA(cudaMemsetAsync(tag, 0, (size_t)N, st));
         PFF_CUDA(cudaMemsetAsync(tag_, 0, (size_t)N, st));
-        if (nonlocal) {
-            // general receivers: the reference's tag propagation by pointer jumping
+        if (general) {
+            // the reference's tag propagation by pointer jumping (:424-435)
             { k_carve_tag_saddles<<<nbk, B, 0, st>>>(basin_saddlenode, tag, N); count_launch(); }
             PFF_CUDA(cudaMemcpyAsync(tag_, tag, (size_t)N, cudaMemcpyDeviceToDevice, st));
             PFF_CUDA(cudaMemcpyAsync(rec, rec_, nb4, cudaMemcpyDeviceToDevice, st));
@@ -1215,8 +1380,11 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
                 { k_carve_it1<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
                 { k_carve_it2<<<nbk, B, 0, st>>>(tag, tag_, rec, rec_, N, r, cflags); count_launch(); }
             }
+            // finalise (:390-403): copy, reversal with the serial last writer, saddle links
             PFF_CUDA(cudaMemcpyAsync(rec, rec__, nb4, cudaMemcpyDeviceToDevice, st));
-            { k_carve_reverse<<<nbk, B, 0, st>>>(rec, rec__, tag, N); count_launch(); }
+            PFF_CUDA(cudaMemsetAsync(w.R, 0xff, nb4, st));  // claims start at -1
+            { k_rev_claim<<<nbk, B, 0, st>>>(rec__, tag, w.R, N); count_launch(); }
+            { k_rev_apply<<<nbk, B, 0, st>>>(rec, w.R, N); count_launch(); }
             { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec, basin_saddlenode, out, N, 0); count_launch(); }
             PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :526
             PFF_TRY(check_cuda("pff_reroute_flow"));
@@ -1240,39 +1408,56 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         PFF_CUDA(cudaStreamSynchronize(st));
         if (h[0]) break;  // walk bounds exceeded: reported below
         const int ndirty = h[1];
-        // a reversed path without an outlet link (only for elevations >= 1e9): the
-        // pit bookkeeping below does not hold, relabel from scratch next iteration
-        const bool inc_ok = (h[2] == 0);
+        if (h[2]) {
+            // a reversed path without an outlet link (elevations >= 1e9 only)
+            general = true;
+            continue;
+        }
         if (it + 1 >= outer) break;  // :500
-        if (inc_ok && nd_next == 0) {
+        // the basin relabelling; a basin chain that does not converge is a cycle
+        int *flags = w.ctr + 256;
+        PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
+        static int coop_relabel = 0;
+        if (!coop_relabel) {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relabel_jump_coop, 256, 0);
+            coop_relabel = nsm * (per < 4 ? per : 4);
+        }
+        int *plist = w.pits[par];
+        void *args[] = {&w.fin, &plist, &np, &flags};
+        PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, st));
+        count_launch();
+        int *cyc = w.ctr + 49;
+        PFF_CUDA(cudaMemsetAsync(cyc, 0, sizeof(int), st));
+        { k_relabel_check<<<grid, B, 0, st>>>(w.fin, out, w.pits[par], np, N, cyc); count_launch(); }
+        int hc = 0;
+        PFF_CUDA(cudaMemcpyAsync(&hc, cyc, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PFF_CUDA(cudaStreamSynchronize(st));
+        if (trace) fprintf(stderr, "[pff reroute]   after carve: next pits %d dirty %d cycle %d\n", nd_next, ndirty, hc);
+        if (hc) {
+            general = true;  // the carve closed a receiver cycle: the reference's path from here on
+            continue;
+        }
+        if (nd_next == 0) {
             ++n_outer;  // the next iteration would count 0 pits, label, then break (:512-514)
             break;      // its labels are reset by basin_id_init (:537) anyway
         }
-        incremental = inc_ok;
-        if (incremental) {
-            int *flags = w.ctr + 256;
-            PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
-            static int coop_relabel = 0;
-            if (!coop_relabel) {
-                int per = 0;
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_relabel_jump_coop, 256, 0);
-                coop_relabel = nsm * (per < 4 ? per : 4);
-            }
-            int *plist = w.pits[par];
-            void *args[] = {&w.fin, &plist, &np, &flags};
-            PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, st));
-            count_launch();
-            { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, N, ((uintptr_t)bid & 15) == 0); count_launch(); }
-            PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, ndirty, st);
-        }
+        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, N, ((uintptr_t)bid & 15) == 0); count_launch(); }
+        PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, ndirty, st);
+        incremental = true;
         PFF_TRY(check_cuda("pff_reroute_flow"));
     }
-    int err = 0;
-    PFF_CUDA(cudaMemcpyAsync(&err, w.ctr + 43, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int err[5] = {0, 0, 0, 0, 0};
+    PFF_CUDA(cudaMemcpyAsync(err, w.ctr + 43, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PFF_TRY(launch_basin_init(bid, g, st));  // :537
     PFF_CUDA(cudaStreamSynchronize(st));
-    if (err) {
-        set_error("pff_reroute_flow: carve walk exceeded its bounds (receiver cycle?)");
+    if (err[0]) {
+        set_error("pff_reroute_flow: carve walk exceeded its bounds");
+        return PFF_ERR_NOCONV;
+    }
+    if (err[4]) {
+        set_error("pff_reroute_flow: a receiver cycle longer than %d cells, or one whose serial labelling does not "
+                  "converge to a single label", CYC_MAX);
         return PFF_ERR_NOCONV;
     }
     if (n_outer_out) *n_outer_out = n_outer;

@@ -56,20 +56,26 @@ class Flooder:
         for _ in range(N):
             self.iteration()
 
-    def run_to_residual(self, tol_ratio=1e-4, max_iter=20000, check_every=1):
-        """Iterate until max|dh|/dt < tol_ratio * precipitation rate or max_iter.
-        Returns (iterations, stop_reason, residual) with stop_reason in
-        {"residual", "max_iter"}; dh is the change of h over one iteration."""
+    def run_to_residual(self, tol_ratio=1e-4, max_iter=20000, return_trace=False):
+        """Iterate until max|dh|/dt < tol_ratio * precipitation rate, or max_iter
+        iterations; dh is the change of h over one whole iteration.  Returns
+        (iterations, stop_reason, residual) with stop_reason "residual" or
+        "max_iter" (and the per-iteration residuals if return_trace)."""
         thr = tol_ratio * self.precipitation_rates
+        trace = torch.zeros(max_iter, dtype=torch.float32, device=self.h.device)
         res = float("inf")
         for it in range(1, max_iter + 1):
-            track = (it % check_every) == 0
-            self.iteration(track_dh=track)
-            if track:
-                res = float(self._dhmax.item()) / cte.DT_HYDRO
-                if res < thr:
-                    return it, "residual", res
-        return max_iter, "max_iter", res
+            self.iteration(track_dh=True)
+            trace[it - 1:it].copy_(self._dhmax)  # on the device: no extra synchronisation
+            # the reroute synchronises the host every iteration anyway: read the residual
+            res = float(self._dhmax.item()) / cte.DT_HYDRO
+            if res < thr:
+                break
+        n = it
+        out = (n, "residual" if res < thr else "max_iter", res)
+        if return_trace:
+            return out + ((trace[:n] / cte.DT_HYDRO).cpu().numpy(),)
+        return out
 
     def set_h(self, val):
         if isinstance(val, torch.Tensor):

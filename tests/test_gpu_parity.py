@@ -288,3 +288,27 @@ def test_accumulate_general_forest(orc, cuda, grid_given):
         Qo, co = orc.accumulate(rcv, w)
         assert np.array_equal(host(cd).view(np.uint32), co)
         assert np.array_equal(host(Qd).view(np.uint32), Qo.view(np.uint32))
+
+
+def test_routing_lakes_4096_bit_exact(orc, cuda):
+    """The full 4096 x 4096 benchmark workload (2000 pits, periodic east-west,
+    carve): rerouted receivers, uint32 counts and weighted Q bit-exact."""
+    import pyfastflow_b200 as pf
+
+    w = synthetic.routing_lakes(4096)
+    z = w["z"]
+    wt = synthetic.lognormal_weights(4096 * 4096, 102)
+    router = pf.flow.FlowRouter(4096, 4096, 30.0, boundary_mode="periodic_EW")
+    router.set_z(z)
+    router.compute_receivers()
+    router.reroute_flow()
+    router.accumulate_weighted_Q(wt)
+    og = orc.Grid(4096, 4096, 1)
+    rcv, _ = orc.compute_receivers(z, og, 30.0)
+    r2, _, _, _, nout = orc.reroute_flow(rcv, z, og)
+    assert router.last_n_outer == nout
+    assert np.array_equal(router.get_receivers().ravel(), r2)
+    Qo, co = orc.accumulate(r2, wt)
+    assert np.array_equal(router.get_counts().ravel(), co)
+    assert np.array_equal(router.get_Q().ravel().view(np.uint32), Qo.view(np.uint32))
+    assert orc.count_cycle_nodes(r2) == 0

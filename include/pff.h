@@ -164,6 +164,36 @@ int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, cons
                         float dx, float dx2, float manning, float edgesw, float dt,
                         const float *h_ref, float *dhmax, void *stream);
 
+/* ---- Ragged batch ----------------------------------------------------------------
+ * Many independent tiles (own nx, ny, dx, boundary mode 0-2) packed back to back,
+ * tile t's cells at [tile_offset[t], tile_offset[t] + nx*ny) in row-major order.
+ * One persistent launch runs, per tile, the chain a FlowRouter user runs tile by
+ * tile: compute_receivers (receivers.py:16-58), reroute_flow(carve=True)
+ * (lakeflow.py:466-538) and accumulate (flowfields.py:254-292, with a per-cell
+ * seed and exact uint32 counts).  No single reference counterpart: the reference
+ * routes one grid per process.  Results are bit-identical to those per-tile calls.
+ *
+ * pff_batch_plan: validates the tiles, fills tile_offset[ntiles] and (optional)
+ * order[ntiles] (the largest-first processing order) and returns the total cell
+ * count; with workspace == NULL it only does that (size query), otherwise it also
+ * uploads the tile table into the workspace (synchronizes `stream`).  Errors are
+ * returned negated (-PFF_ERR_*).
+ * pff_batch_route: asynchronous launch on `stream`, no host synchronisation, so it
+ * can be captured in a CUDA graph.  Q: per-cell seed in, upstream sum out.
+ * threads: 256, 512 or 1024 per CTA; ctas_per_sm is clamped to the occupancy.
+ * pff_batch_status: error bits of the last launch (synchronizes `stream`):
+ * 1 = a tile mode outside 0-2, 8 = cells of one receiver cycle ended with
+ * different serial labels, 16 = a carve did not converge. */
+size_t pff_batch_workspace_bytes(long long total_cells, int ntiles);
+long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_ny, const int32_t *tile_mode,
+                         const float *tile_dx, int ntiles, long long *tile_offset, int32_t *order,
+                         void *workspace, size_t workspace_bytes, void *stream);
+int pff_batch_route(const float *z, int32_t *receivers, float *gradient, float *Q, uint32_t *counts,
+                    long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
+                    size_t workspace_bytes, void *stream);
+int pff_batch_status(long long total_cells, int ntiles, void *workspace, size_t workspace_bytes,
+                     int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

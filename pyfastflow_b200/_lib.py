@@ -39,6 +39,10 @@ SIGNATURES = {
     "pff_diffuse_workspace_bytes": (_sz, [_i32]),
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
+    "pff_batch_workspace_bytes": (_sz, [_i64, _i32]),
+    "pff_batch_plan": (_i64, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
+    "pff_batch_route": (_i32, [_vp] * 5 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),
+    "pff_batch_status": (_i32, [_i64, _i32, _vp, _sz, C.POINTER(C.c_int), _vp]),
 }
 
 _lib = None

@@ -1,0 +1,736 @@
+// libpff ragged batch: hundreds of independent DEM tiles of uneven sizes routed
+// (receivers -> carve reroute -> accumulate) in ONE persistent launch over a packed
+// layout.  Each CTA takes whole tiles from a queue (largest first) and runs the
+// entire chain for its tile with block-wide barriers between passes: tiles are
+// independent, so nothing synchronises across CTAs and the launch needs no host
+// round trip (it can be captured in a CUDA graph).
+//
+// Within a tile the steps are the reference's own (pyfastflow/flow/receivers.py:31-58,
+// lakeflow.py:466-538, downstream_propag.py:59-179, flowfields.py:254-292) with the
+// pinned semantics of the single-grid path: serial last writer for the saddle node
+// and for path reversal (largest index), the serial 2-cycle pass, serial labelling of
+// receiver cycles (emulated), snapshot rake-and-compress rounds with donors in
+// ascending index.  Results are bit-identical to routing each tile on its own.
+#include <algorithm>
+#include "pff_internal.h"
+
+namespace pff {
+
+struct BatchTile {
+    long long off;   // first cell of the tile in the packed arrays
+    long long boff;  // first basin entry (N+1 entries per tile)
+    int nx, ny, mode;
+    float dx;
+};
+
+// Packed per-cell and per-basin arrays of the batch (device pointers).
+struct BatchArrays {
+    const float *z;
+    int32_t *rcv;      // out: rerouted receivers (tile-local indices)
+    float *grad;       // out: steepest gradient of the original receivers
+    float *Q;          // in: per-cell seed, out: upstream sum
+    uint32_t *counts;  // out: upstream cell counts
+    int32_t *rec_, *rec__, *bid, *mark;
+    float *zp;
+    uint8_t *isb, *tag, *tag_;
+    long long *saddle, *outlet;  // N+1 per tile
+    int32_t *snode;              // N+1 per tile
+    uint8_t *inv;                // N+1 per tile
+    int32_t *dnr, *dnr_;         // 4 per cell
+    int32_t *ndnr, *ndnr_, *src;
+    float *p_;
+    uint32_t *c_;
+    const BatchTile *tiles;  // in largest-first order
+    int *queue;              // [0] next tile
+    int *status;             // [0] error bits (see pff_batch_status)
+};
+
+enum : int { BST_MODE = 1, BST_CYCLE_LABELS = 8, BST_CARVE = 16 };
+
+struct BatchShm {
+    int red;
+    int cur;
+    int ws[32];
+};
+
+__device__ __forceinline__ int bceil_log2(long long n)
+{
+    int r = 0;
+    long long p = 1;
+    while (p < n) { p <<= 1; ++r; }
+    return r;
+}
+
+__device__ __forceinline__ long long inv_key() { return pack_key(1e8f, 42); }
+
+// Block-wide sum (every thread gets it).
+__device__ __forceinline__ int bsum(int v, BatchShm &sh)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) sh.red = 0;
+    __syncthreads();
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh.red, v);
+    __syncthreads();
+    const int r = sh.red;
+    __syncthreads();
+    return r;
+}
+
+// Block-wide exclusive prefix sum of v (blockDim a multiple of 32); *total = sum.
+__device__ __forceinline__ int bscan(int v, BatchShm &sh, int *total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) sh.ws[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = lane < nw ? sh.ws[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) sh.ws[lane] = s;
+    }
+    __syncthreads();
+    const int before = (wid ? sh.ws[wid - 1] : 0) + x - v;
+    *total = sh.ws[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+#define FOR_CELLS(i, N) for (int i = threadIdx.x; i < (N); i += blockDim.x)
+
+template <int MODE>
+__device__ __forceinline__ bool leave(const Grid &g, int i)
+{
+    return can_leave_i<MODE>(g, i);
+}
+
+// ---- labels: basin_id_init + propagate_basin on a copy of rec_ (lakeflow.py:47-80, 507-511)
+//
+// Acyclic receivers: the fixed point of pointer jumping, reached in parallel.  On a
+// receiver cycle the reference's serial in-place rounds give a result that depends
+// only on the cycle's cells visited in ascending index; it is emulated here and every
+// cell draining into the cycle takes the cycle's label.
+template <int MODE>
+__device__ void tile_labels(const Grid &g, int N, const int32_t *rec_, int32_t *work, int32_t *bid, int32_t *mark,
+                            int32_t *scr, int rounds, BatchShm &sh, int *status)
+{
+    FOR_CELLS(i, N) {
+        bid[i] = leave<MODE>(g, i) ? 0 : i + 1;
+        work[i] = rec_[i];
+        mark[i] = 0;
+    }
+    __syncthreads();
+    for (int r = 0; r < rounds; ++r) {
+        int ch = 0;
+        FOR_CELLS(i, N) {
+            const int p = work[i];
+            const int b = bid[p], pp = work[p];
+            if (bid[i] != b) { bid[i] = b; ch = 1; }
+            if (pp != p) { work[i] = pp; ch = 1; }
+        }
+        if (!__syncthreads_or(ch)) break;
+    }
+    // After the rounds every pointer sits on a true root or on a cycle cell.
+    int unresolved = 0;
+    FOR_CELLS(i, N) {
+        const int x = work[i];
+        unresolved |= (rec_[x] != x);
+    }
+    if (!__syncthreads_or(unresolved)) return;
+    // Mark every cycle cell: walkers claim cells and stop at the first cell another
+    // walker claimed, which covers each cycle exactly once.
+    FOR_CELLS(i, N) {
+        int x = work[i];
+        if (rec_[x] == x) continue;
+        for (int s = 0; s <= N; ++s) {
+            if (atomicExch(mark + x, 1)) break;
+            x = rec_[x];
+        }
+    }
+    __syncthreads();
+    // cycle cells in ascending index order: cells[a], pos[cell] = a
+    int32_t *cells = scr, *pos = scr + N, *lrec = scr + 2LL * N, *lb = scr + 3LL * N;
+    int L = 0;
+    for (int base = 0; base < N; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int f = (i < N && mark[i]) ? 1 : 0;
+        int tot;
+        const int p = bscan(f, sh, &tot);
+        if (f) { cells[L + p] = i; pos[i] = L + p; }
+        L += tot;
+    }
+    __syncthreads();
+    FOR_CELLS(a, L) {
+        const int c = cells[a];
+        lrec[a] = pos[rec_[c]];
+        lb[a] = leave<MODE>(g, c) ? 0 : c + 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int r = 0; r < rounds; ++r)
+            for (int a = 0; a < L; ++a) {
+                lb[a] = lb[lrec[a]];
+                lrec[a] = lrec[lrec[a]];
+            }
+    __syncthreads();
+    int bad = 0;
+    FOR_CELLS(a, L) bad |= (lb[a] != lb[pos[rec_[cells[a]]]]);  // one label per cycle
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, BST_CYCLE_LABELS);
+    FOR_CELLS(i, N) {
+        const int x = work[i];
+        if (rec_[x] != x) bid[i] = lb[pos[x]];
+    }
+    __syncthreads();
+}
+
+// ---- saddlesort passes 1-5 (lakeflow.py:106-281) ------------------------------------
+template <int MODE>
+__device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_t *isb, float *zp, long long *sad,
+                                int32_t *snode, long long *out, uint8_t *inv, const float *z)
+{
+    const long long iv = inv_key();
+    FOR_CELLS(b, N + 1) {
+        sad[b] = iv;
+        out[b] = iv;
+        snode[b] = -1;
+        inv[b] = 0;
+    }
+    __syncthreads();
+    // passes 1 and 2: z' and the per-basin lowest packed (z', neighbour basin)
+    FOR_CELLS(i, N) {
+        const float zi = z[i];
+        if (leave<MODE>(g, i)) {
+            zp[i] = zi;
+            isb[i] = 0;  // never written by the reference: its zero initial value
+            continue;
+        }
+        const int row = i / g.nx, col = i - row * g.nx;
+        const int bi = bid[i];
+        int js[4];
+        neighbours4<MODE>(g, i, row, col, js);
+        bool border = false;
+        float zn = 1e9f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (js[k] != -1 && bid[js[k]] != bi) {
+                border = true;
+                zn = fminf(zn, z[js[k]]);
+            }
+        isb[i] = border;
+        const float zpi = border ? fmaxf(zi, zn) : 1e9f;
+        zp[i] = zpi;
+        if (!border) continue;
+        long long res = iv;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (js[k] == -1) continue;
+            const int bj = bid[js[k]];
+            if (bj != bi) {
+                const long long c = pack_key(zpi, bj);
+                res = c < res ? c : res;
+            }
+        }
+        if (res != iv) atomicMin(sad + bi, res);
+    }
+    __syncthreads();
+    // pass 3: saddle node = largest qualifying index (serial last writer)
+    FOR_CELLS(i, N) {
+        if (!isb[i]) continue;
+        const int bi = bid[i];
+        if (bi == 0) continue;
+        const long long s = sad[bi];
+        const float tz = key_value(s);
+        const int tb = key_index(s);
+        const float zpi = zp[i];
+        const int row = i / g.nx, col = i - row * g.nx;
+        int js[4];
+        neighbours4<MODE>(g, i, row, col, js);
+        bool here = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (js[k] != -1 && bid[js[k]] == tb && zpi == tz) here = true;
+        if (here) atomicMax(snode + bi, i);
+    }
+    __syncthreads();
+    // pass 4: outlet = lowest foreign neighbour of the saddle node (first k wins)
+    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x) {
+        if (sad[b] == iv) continue;
+        const int node = snode[b];
+        if (node < 0) continue;
+        float tz = 1e9f;
+        int r = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = neighbour_i<MODE>(g, node, k);
+            if (j == -1) continue;
+            const float zj = z[j];
+            if (bid[j] != b && tz > zj) {
+                tz = zj;
+                r = j;
+            }
+        }
+        if (r > -1) out[b] = pack_key(tz, r);
+    }
+    __syncthreads();
+    // pass 5: 2-cycles b -> b' -> b with b' < b, snapshot reads, plus the one basin
+    // (bid[42]) whose serial outcome can differ from the snapshot
+    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x) {
+        const long long ob = out[b];
+        if (ob == iv) continue;
+        const int bd1 = bid[key_index(ob)];
+        if (bd1 == 0) continue;
+        const int ro2 = key_index(out[bd1]);
+        const int bd2 = (ro2 >= 0 && ro2 < N) ? bid[ro2] : -1;
+        if (bd2 == b && bd1 < b) inv[b] = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && N > 42) {
+        const int D = bid[42];
+        if (D > 0 && D < N && out[D] != iv) {
+            const int bd1 = bid[key_index(out[D])];
+            if (bd1 != 0 && bd1 < D && inv[bd1]) inv[D] = 1;
+        }
+    }
+    __syncthreads();
+    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x)
+        if (inv[b]) {
+            out[b] = iv;
+            sad[b] = iv;
+            snode[b] = -1;
+        }
+    __syncthreads();
+}
+
+// ---- reroute_carve (lakeflow.py:308-438); leaves the result in rec and rec_ ----------
+__device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *rec__, int32_t *claim, uint8_t *tag,
+                           uint8_t *tag_, const int32_t *snode, const long long *out, int *status)
+{
+    const long long iv = inv_key();
+    FOR_CELLS(i, N) {
+        tag[i] = 0;
+        claim[i] = -1;
+    }
+    __syncthreads();
+    FOR_CELLS(b, N) {
+        const int s = snode[b];
+        if (s != -1) tag[s] = 1;
+    }
+    __syncthreads();
+    FOR_CELLS(i, N) {
+        tag_[i] = tag[i];
+        const int r = rec_[i];
+        rec[i] = r;
+        rec__[i] = r;
+    }
+    __syncthreads();
+    // until no tag changes; each productive round adds a tag, so N + 1 rounds bound it
+    int r = 0;
+    for (; r <= N + 1; ++r) {
+        FOR_CELLS(i, N) {
+            const int ri = rec[i];
+            if (tag[i]) tag_[ri] = 1;
+            rec_[i] = ri;
+        }
+        __syncthreads();
+        int ch = 0;
+        FOR_CELLS(i, N) {
+            rec[i] = rec_[rec_[i]];
+            const uint8_t t = tag_[i];
+            if (tag[i] != t) {
+                ch = 1;
+                tag[i] = t;
+            }
+        }
+        if (!__syncthreads_or(ch)) break;
+    }
+    if (r > N + 1 && threadIdx.x == 0) atomicOr(status, BST_CARVE);
+    // finalise: pre-carve receivers, path reversal (largest index wins), saddle links
+    FOR_CELLS(i, N) {
+        const int r0 = rec__[i];
+        rec[i] = r0;
+        if (tag[r0] && tag[i] && i != r0) atomicMax(claim + r0, i);
+    }
+    __syncthreads();
+    FOR_CELLS(x, N) {
+        const int c = claim[x];
+        if (c >= 0) rec[x] = c;
+    }
+    __syncthreads();
+    FOR_CELLS(b, N) {
+        const long long ob = out[b];
+        if (ob != iv) rec[snode[b]] = key_index(ob);
+    }
+    __syncthreads();
+    FOR_CELLS(i, N) rec_[i] = rec[i];
+    __syncthreads();
+}
+
+// ---- rake-and-compress (downstream_propag.py:21-179), f32 and u32 payloads ---------------
+__device__ __forceinline__ bool bget_src(const int32_t *src, int t, int it)
+{
+    const int e = src[t];
+    bool flip = e < 0;
+    if (abs(e) == it + 1) flip = !flip;
+    return flip;
+}
+
+__device__ void tile_accumulate(int N, const int32_t *rcv, float *p, uint32_t *c, int32_t *dnr, int32_t *dnr_,
+                                int32_t *ndnr, int32_t *ndnr_, int32_t *src, float *p_, uint32_t *c_)
+{
+    FOR_CELLS(t, N) {
+        ndnr[t] = 0;
+        src[t] = 0;
+        c[t] = 1u;
+    }
+    __syncthreads();
+    FOR_CELLS(t, N) {  // rcv2donor (:78-96); D4 receivers give at most 4 donors
+        const int r = rcv[t];
+        if (r == t) continue;
+        const int slot = atomicAdd(ndnr + r, 1);
+        if (slot < 4) dnr[4LL * r + slot] = t;
+    }
+    __syncthreads();
+    FOR_CELLS(r, N) {  // ascending donor index: the reference's serial slot order
+        const int n = min(ndnr[r], 4);
+        int *d = dnr + 4LL * r;
+        for (int a = 1; a < n; ++a) {
+            const int x = d[a];
+            int b = a - 1;
+            while (b >= 0 && d[b] > x) {
+                d[b + 1] = d[b];
+                --b;
+            }
+            d[b + 1] = x;
+        }
+    }
+    __syncthreads();
+    const int logn = bceil_log2(N) + 1;
+    for (int it = 0; it <= logn; ++it) {
+        int worked_any = 0;
+        FOR_CELLS(tid, N) {
+            const bool flip = bget_src(src, tid, it);
+            int todo = flip ? ndnr_[tid] : ndnr[tid];
+            if (todo <= 0) continue;
+            const long long base = 4LL * tid;
+            int donors[4] = {-1, -1, -1, -1};
+            bool worked = false;
+            float padd = 0.f;
+            uint32_t cadd = 0;
+            int i = 0;
+            while (i < todo && i < 4) {
+                if (donors[i] == -1) donors[i] = flip ? dnr_[base + i] : dnr[base + i];
+                const int did = donors[i];
+                const bool fd = bget_src(src, did, it);
+                const int nd = fd ? ndnr_[did] : ndnr[did];
+                if (nd <= 1) {
+                    if (!worked) {
+                        padd = flip ? p_[tid] : p[tid];
+                        cadd = flip ? c_[tid] : c[tid];
+                    }
+                    worked = true;
+                    padd = __fadd_rn(padd, fd ? p_[did] : p[did]);
+                    cadd += fd ? c_[did] : c[did];
+                    if (nd == 0) {
+                        --todo;
+                        if (todo > i) donors[i] = flip ? dnr_[base + todo] : dnr[base + todo];
+                        --i;
+                    } else {
+                        donors[i] = fd ? dnr_[4LL * did] : dnr[4LL * did];
+                    }
+                }
+                ++i;
+            }
+            if (!worked) continue;
+            worked_any = 1;
+            const int m = todo < 4 ? todo : 4;
+            if (flip) {
+                ndnr[tid] = todo;
+                p[tid] = padd;
+                c[tid] = cadd;
+                for (int j = 0; j < m; ++j) dnr[base + j] = donors[j];
+            } else {
+                ndnr_[tid] = todo;
+                p_[tid] = padd;
+                c_[tid] = cadd;
+                for (int j = 0; j < m; ++j) dnr_[base + j] = donors[j];
+            }
+            src[tid] = (flip ? 1 : -1) * (it + 1);
+        }
+        // a round in which nothing worked leaves the state, and every later round, unchanged
+        if (!__syncthreads_or(worked_any)) break;
+    }
+    FOR_CELLS(t, N) {  // fuse(Q, src, Q_, logn)
+        if (bget_src(src, t, logn)) {
+            p[t] = p_[t];
+            c[t] = c_[t];
+        }
+    }
+    __syncthreads();
+}
+
+template <int MODE>
+__device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &sh)
+{
+    const Grid g{T.nx, T.ny, MODE, nullptr};
+    const int N = T.nx * T.ny;
+    const long long o = T.off, ob = T.boff;
+    const float *z = A.z + o;
+    int32_t *rec = A.rcv + o, *rec_ = A.rec_ + o, *rec__ = A.rec__ + o, *bid = A.bid + o;
+    const int lrounds = bceil_log2(N) + 1;
+
+    // receivers (receivers.py:31-58): strict >, first k wins ties
+    FOR_CELLS(i, N) {
+        const int row = i / T.nx, col = i - row * T.nx;
+        int js[4];
+        neighbours4<MODE>(g, i, row, col, js);
+        const float zi = z[i];
+        int r = i;
+        float sr = 0.f, dbest = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (js[k] == -1) continue;
+            const float d = __fsub_rn(zi, z[js[k]]);
+            if (d > dbest) {  // a smaller difference cannot give a larger quotient
+                const float q = __fdiv_rn(d, T.dx);
+                if (q > sr) {
+                    sr = q;
+                    r = js[k];
+                    dbest = d;
+                }
+            }
+        }
+        rec[i] = r;
+        rec_[i] = r;
+        A.grad[o + i] = sr;
+    }
+    __syncthreads();
+
+    // reroute_flow(carve=True) (lakeflow.py:466-538)
+    int np = 0;
+    FOR_CELLS(i, N) np += (rec_[i] == i && !leave<MODE>(g, i));
+    const int ndep = bsum(np, sh);
+    if (ndep > 0) {
+        const int outer = bceil_log2(ndep) + 1;
+        for (int it = 0; it < outer; ++it) {
+            int nb = 0;
+            if (it > 0) FOR_CELLS(i, N) nb += (rec_[i] == i && !leave<MODE>(g, i));
+            const int nd = it > 0 ? bsum(nb, sh) : ndep;
+            if (nd == 0) break;  // (the labels the reference computes first are overwritten)
+            tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
+            tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
+                                  A.inv + ob, z);
+            tile_carve(N, rec, rec_, rec__, A.mark + o, A.tag + o, A.tag_ + o, A.snode + ob, A.outlet + ob,
+                       A.status);
+        }
+    }
+
+    // accumulate: Q holds the seed (flowfields.py:272-292)
+    tile_accumulate(N, rec, A.Q + o, A.counts + o, A.dnr + 4 * o, A.dnr_ + 4 * o, A.ndnr + o, A.ndnr_ + o, A.src + o,
+                    A.p_ + o, A.c_ + o);
+}
+
+// Persistent: each CTA takes the next tile (largest first) until the queue is empty.
+__global__ void __launch_bounds__(1024) k_batch_route(int ntiles, BatchArrays A)
+{
+    __shared__ BatchShm sh;
+    for (;;) {
+        if (threadIdx.x == 0) sh.cur = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int k = sh.cur;
+        __syncthreads();
+        if (k >= ntiles) return;
+        const BatchTile T = A.tiles[k];
+        switch (T.mode) {
+        case 0: route_tile<0>(T, A, sh); break;
+        case 1: route_tile<1>(T, A, sh); break;
+        case 2: route_tile<2>(T, A, sh); break;
+        default:
+            if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
+            break;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_batch_reset(int *ctr)
+{
+    ctr[0] = 0;
+    ctr[1] = 0;
+}
+
+// Workspace layout, identical for the plan and the launches.
+struct BatchWs {
+    BatchArrays A;
+    BatchTile *tiles;
+    int *ctr;
+    bool ok;
+};
+
+static BatchWs carve_batch(void *ws, size_t wsb, long long total, int ntiles)
+{
+    Carver cv(ws, wsb);
+    const size_t n = (size_t)total, nb = n + (size_t)ntiles;
+    BatchWs w{};
+    BatchArrays &A = w.A;
+    w.ctr = cv.take<int>(64);
+    w.tiles = cv.take<BatchTile>((size_t)ntiles);
+    A.rec_ = cv.take<int32_t>(n);
+    A.rec__ = cv.take<int32_t>(n);
+    A.bid = cv.take<int32_t>(n);
+    A.mark = cv.take<int32_t>(n);
+    A.zp = cv.take<float>(n);
+    A.isb = cv.take<uint8_t>(n);
+    A.tag = cv.take<uint8_t>(n);
+    A.tag_ = cv.take<uint8_t>(n);
+    A.saddle = cv.take<long long>(nb);
+    A.outlet = cv.take<long long>(nb);
+    A.snode = cv.take<int32_t>(nb);
+    A.inv = cv.take<uint8_t>(nb);
+    A.dnr = cv.take<int32_t>(4 * n);
+    A.dnr_ = cv.take<int32_t>(4 * n);
+    A.ndnr = cv.take<int32_t>(n);
+    A.ndnr_ = cv.take<int32_t>(n);
+    A.src = cv.take<int32_t>(n);
+    A.p_ = cv.take<float>(n);
+    A.c_ = cv.take<uint32_t>(n);
+    A.tiles = w.tiles;
+    A.queue = w.ctr;
+    A.status = w.ctr + 1;
+    w.ok = A.c_ != nullptr;
+    return w;
+}
+
+}  // namespace pff
+
+using namespace pff;
+
+extern "C" size_t pff_batch_workspace_bytes(long long total_cells, int ntiles)
+{
+    if (total_cells <= 0 || ntiles <= 0) return 0;
+    const size_t n = (size_t)total_cells, nb = n + (size_t)ntiles;
+    return Carver::round(64 * 4) + Carver::round(sizeof(BatchTile) * (size_t)ntiles) + Carver::round(4 * n) * 5 +
+           Carver::round(n) * 3 + Carver::round(8 * nb) * 2 + Carver::round(4 * nb) + Carver::round(nb) +
+           Carver::round(16 * n) * 2 + Carver::round(4 * n) * 5 + 256;
+}
+
+namespace pff {
+static int batch_check(long long total, int ntiles, void *ws, size_t wsb, const char *who)
+{
+    if (ntiles <= 0 || total <= 0) {
+        set_error("%s: empty batch", who);
+        return PFF_ERR_ARG;
+    }
+    if (!ws || wsb < pff_batch_workspace_bytes(total, ntiles)) {
+        set_error("%s: workspace too small", who);
+        return PFF_ERR_WORKSPACE;
+    }
+    return PFF_OK;
+}
+}  // namespace pff
+
+extern "C" long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_ny, const int32_t *tile_mode,
+                                    const float *tile_dx, int ntiles, long long *tile_offset, int32_t *order,
+                                    void *workspace, size_t workspace_bytes, void *stream)
+{
+    clear_error();
+    if (ntiles <= 0 || !tile_nx || !tile_ny || !tile_mode || !tile_dx || !tile_offset) {
+        set_error("pff_batch_plan: bad arguments");
+        return -PFF_ERR_ARG;
+    }
+    long long off = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        const int nx = tile_nx[t], ny = tile_ny[t], md = tile_mode[t];
+        if (nx < 2 || ny < 2 || md < 0 || md > 2 || (long long)nx * ny * 4 >= (1LL << 31) ||
+            !(tile_dx[t] > 0.f)) {
+            set_error("pff_batch_plan: tile %d: bad size %dx%d, mode %d or dx (modes 0-2 are batched)", t, nx, ny,
+                      md);
+            return -PFF_ERR_ARG;
+        }
+        tile_offset[t] = off;
+        off += (long long)nx * ny;
+    }
+    const long long total = off;
+    if (!workspace) return total;  // size query
+    const int rc = batch_check(total, ntiles, workspace, workspace_bytes, "pff_batch_plan");
+    if (rc) return -rc;
+    // largest tiles first (longest-processing-time order); equal sizes by tile index
+    int *ord = new int[ntiles];
+    for (int t = 0; t < ntiles; ++t) ord[t] = t;
+    auto cells = [&](int t) { return (long long)tile_nx[t] * tile_ny[t]; };
+    std::stable_sort(ord, ord + ntiles, [&](int a, int b) { return cells(a) > cells(b); });
+    BatchTile *ht = new BatchTile[ntiles];
+    for (int k = 0; k < ntiles; ++k) {
+        const int t = ord[k];
+        ht[k] = BatchTile{tile_offset[t], tile_offset[t] + t, tile_nx[t], tile_ny[t], tile_mode[t], tile_dx[t]};
+        if (order) order[k] = t;
+    }
+    BatchWs w = carve_batch(workspace, workspace_bytes, total, ntiles);
+    cudaStream_t st = S(stream);
+    const cudaError_t e1 = cudaMemcpyAsync(w.tiles, ht, sizeof(BatchTile) * ntiles, cudaMemcpyHostToDevice, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);  // the host array must outlive the copy
+    delete[] ht;
+    delete[] ord;
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        set_error("pff_batch_plan: descriptor upload: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        return -PFF_ERR_CUDA;
+    }
+    return total;
+}
+
+extern "C" int pff_batch_route(const float *z, int32_t *receivers, float *gradient, float *Q, uint32_t *counts,
+                               long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
+                               size_t workspace_bytes, void *stream)
+{
+    clear_error();
+    PFF_TRY(batch_check(total_cells, ntiles, workspace, workspace_bytes, "pff_batch_route"));
+    if (!z || !receivers || !gradient || !Q || !counts) {
+        set_error("pff_batch_route: null pointer");
+        return PFF_ERR_ARG;
+    }
+    if (threads != 256 && threads != 512 && threads != 1024) {
+        set_error("pff_batch_route: threads must be 256, 512 or 1024 (got %d)", threads);
+        return PFF_ERR_ARG;
+    }
+    int dev = 0, nsm = 148, occ = 1;
+    PFF_CUDA(cudaGetDevice(&dev));
+    PFF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PFF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_route, threads, 0));
+    if (ctas_per_sm < 1) ctas_per_sm = 1;
+    if (ctas_per_sm > occ) ctas_per_sm = occ > 0 ? occ : 1;
+    BatchWs w = carve_batch(workspace, workspace_bytes, total_cells, ntiles);
+    BatchArrays A = w.A;
+    A.z = z;
+    A.rcv = receivers;
+    A.grad = gradient;
+    A.Q = Q;
+    A.counts = counts;
+    cudaStream_t st = S(stream);
+    const int grid = std::min(nsm * ctas_per_sm, ntiles);
+    { k_batch_reset<<<1, 1, 0, st>>>(w.ctr); count_launch(); }
+    { k_batch_route<<<grid, threads, 0, st>>>(ntiles, A); count_launch(); }
+    return check_cuda("pff_batch_route");
+}
+
+extern "C" int pff_batch_status(long long total_cells, int ntiles, void *workspace, size_t workspace_bytes,
+                                int *status, void *stream)
+{
+    clear_error();
+    PFF_TRY(batch_check(total_cells, ntiles, workspace, workspace_bytes, "pff_batch_status"));
+    if (!status) {
+        set_error("pff_batch_status: null pointer");
+        return PFF_ERR_ARG;
+    }
+    BatchWs w = carve_batch(workspace, workspace_bytes, total_cells, ntiles);
+    cudaStream_t st = S(stream);
+    PFF_CUDA(cudaMemcpyAsync(status, w.A.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PFF_CUDA(cudaStreamSynchronize(st));
+    return PFF_OK;
+}

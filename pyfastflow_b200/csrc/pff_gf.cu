@@ -37,7 +37,7 @@ __global__ void k_fill_apply(float *zh, float *h, const float *__restrict__ z_, 
 // Per-cell outgoing weights fl(tS_k / sums) and a "source" flag (non-outlet
 // with sums != 0), computed once per call: zh does not change between sweeps.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_diffuse_weights(const float *__restrict__ zh, float4 *w, uint8_t *issrc,
+__global__ void __launch_bounds__(256) k_diffuse_weights(const float *__restrict__ zh, float *w, uint8_t *issrc,
                                                          Grid g, float dx)
 {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -58,32 +58,46 @@ __global__ void __launch_bounds__(256) k_diffuse_weights(const float *__restrict
     }
     if (sums == 0.f) { issrc[i] = 0; return; }
     issrc[i] = 1;
-    w[i] = make_float4(__fdiv_rn(s[0], sums), __fdiv_rn(s[1], sums), __fdiv_rn(s[2], sums), __fdiv_rn(s[3], sums));
+    // one plane per direction k: a gather reads only the weight it needs
+    const size_t N = (size_t)g.N();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k * N + i] = __fdiv_rn(s[k], sums);
 }
 
 // One sweep in gather form: temp[j] = P*dx^2 + sum over sources i ascending, then
 // k ascending, of fl(w_ik * Q[i]) -- the serial order of the reference's atomics.
+// Interior cells of modes 0-2: the sources are the top, left, right and bottom
+// neighbours (ascending index), each reaching j through its bottom, right, left
+// and top link respectively.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__ Q, float *__restrict__ Qn,
-                                                       const float4 *__restrict__ w, const uint8_t *__restrict__ issrc,
+                                                       const float *__restrict__ w, const uint8_t *__restrict__ issrc,
                                                        Grid g, float prec_dx2)
 {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     const int row = blockIdx.y * blockDim.y + threadIdx.y;
     if (col >= g.nx || row >= g.ny) return;
     const int j = row * g.nx + col;
+    const size_t N = (size_t)g.N();
+    float acc = prec_dx2;
+    if (MODE != 3 && row > 0 && row < g.ny - 1 && col > 0 && col < g.nx - 1) {
+        const int nx = g.nx;
+        if (issrc[j - nx]) acc = __fadd_rn(acc, __fmul_rn(w[3 * N + j - nx], Q[j - nx]));
+        if (issrc[j - 1]) acc = __fadd_rn(acc, __fmul_rn(w[2 * N + j - 1], Q[j - 1]));
+        if (issrc[j + 1]) acc = __fadd_rn(acc, __fmul_rn(w[1 * N + j + 1], Q[j + 1]));
+        if (issrc[j + nx]) acc = __fadd_rn(acc, __fmul_rn(w[j + nx], Q[j + nx]));
+        Qn[j] = acc;
+        return;
+    }
     int c[8];
     const int n = donor_candidates(g, j, row, col, c);
-    float acc = prec_dx2;
     for (int a = 0; a < n; ++a) {
         const int i = c[a];
         if (!issrc[i]) continue;
         const float qi = Q[i];
-        const float4 wi = w[i];
-        const float ww[4] = {wi.x, wi.y, wi.z, wi.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            if (neighbour_i<MODE>(g, i, k) == j) acc = __fadd_rn(acc, __fmul_rn(ww[k], qi));
+            if (neighbour_i<MODE>(g, i, k) == j) acc = __fadd_rn(acc, __fmul_rn(w[k * N + i], qi));
     }
     Qn[j] = acc;
 }
@@ -114,12 +128,6 @@ __global__ void __launch_bounds__(256) k_core1(float *h, const float *__restrict
     dh[i] = tdh;
 }
 
-__device__ __forceinline__ void atomic_max_abs(float *dst, float v)
-{
-    // |v| >= 0 (or NaN, whose bits exceed +inf): unsigned compare orders them.
-    atomicMax(reinterpret_cast<unsigned int *>(dst), __float_as_uint(fabsf(v)));
-}
-
 __global__ void __launch_bounds__(256) k_core2(float *h, float *zh, const float *__restrict__ dh,
                                                const float *__restrict__ href, float *dhmax, int N)
 {
@@ -133,14 +141,22 @@ __global__ void __launch_bounds__(256) k_core2(float *h, float *zh, const float 
         if (dhmax && href) m = fabsf(__fsub_rn(hn, href[i]));
     }
     if (!dhmax || !href) return;
-    // warp max then one atomic per warp
+    // |dh| >= 0 or NaN: as unsigned bits, NaN sorts above every finite value;
+    // warp max, block max, then one atomic per block
     unsigned mu = __float_as_uint(m);
     for (int o = 16; o; o >>= 1) mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
-    if ((threadIdx.x & 31) == 0 && mu) atomicMax(reinterpret_cast<unsigned int *>(dhmax), mu);
+    __shared__ unsigned wm[8];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mu;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned b = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) b = max(b, wm[k]);
+        if (b) atomicMax(reinterpret_cast<unsigned int *>(dhmax), b);
+    }
 }
 
 template <int MODE>
-static void l_diffuse(const float *zh, float *Q, float *temp, float4 *w, uint8_t *issrc, int nsweeps,
+static void l_diffuse(const float *zh, float *Q, float *temp, float *w, uint8_t *issrc, int nsweeps,
                       const Grid &g, float dx, float prec_dx2, cudaStream_t st)
 {
     dim3 b(32, 8), gr(div_up(g.nx, 32), div_up(g.ny, 8));
@@ -265,7 +281,7 @@ extern "C" int pff_fill_z_add_delta_noalloc(float *zh, float *h, float *z_, cons
 
 extern "C" size_t pff_diffuse_workspace_bytes(int N)
 {
-    return Carver::round(sizeof(float4) * (size_t)N) + Carver::round((size_t)N) + 512;
+    return Carver::round(sizeof(float) * 4 * (size_t)N) + Carver::round((size_t)N) + 512;
 }
 
 extern "C" int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps, int nx, int ny, float dx,
@@ -284,7 +300,7 @@ extern "C" int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps
     Grid g{nx, ny, bound_mode, codes};
     cudaStream_t st = S(stream);
     Carver cv(workspace, workspace_bytes);
-    float4 *w = cv.take<float4>(N);
+    float *w = cv.take<float>(4 * (size_t)N);
     uint8_t *issrc = cv.take<uint8_t>(N);
     PFF_MODE_DISPATCH(bound_mode, l_diffuse, zh, Q, temp, w, issrc, nsweeps, g, dx, prec_dx2, st);
     // the reference ends each sweep with Q == temp (:74-75)

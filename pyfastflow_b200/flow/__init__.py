@@ -11,11 +11,13 @@ from .lakeflow import depression_counter, basin_identification, saddlesort, rero
 from .f32_i32_struct import pack_float_index, unpack_float_index
 from .fill_topo import fill_z_add_delta
 from .flowfields import FlowRouter
-from . import environment, receivers, downstream_propag, lakeflow, f32_i32_struct, fill_topo, flowfields
+from .ragged import RaggedRouter
+from . import environment, receivers, downstream_propag, lakeflow, f32_i32_struct, fill_topo, flowfields, ragged
 
 __all__ = [
     "environment", "receivers", "downstream_propag", "lakeflow", "f32_i32_struct", "fill_topo", "flowfields",
-    "FlowRouter", "compute_receivers", "rcv2donor", "rake_compress_accum", "fuse", "depression_counter",
+    "ragged",
+    "FlowRouter", "RaggedRouter", "compute_receivers", "rcv2donor", "rake_compress_accum", "fuse", "depression_counter",
     "basin_identification", "saddlesort", "reroute_flow", "fill_z_add_delta", "pack_float_index",
     "unpack_float_index", "initialise", "reboot",
 ]

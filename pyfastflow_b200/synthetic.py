@@ -79,3 +79,23 @@ def graphflood_plain(n: int = 2048, seed: int = 3):
     npits = int(round(2000 * (n * n) / (4096.0 * 4096.0)))
     return dict(z=spectral_dem(n, n, seed, relief=1500.0, dx=10.0, npits=max(npits, 1)), nx=n, ny=n,
                 dx=10.0, mode="normal")
+
+
+def ragged_tiles(ntiles: int = 512, seed: int = 4, side_min: int = 128, side_max: int = 1024,
+                 max_pits: int = 200, dx: float = 30.0, relief: float = 500.0):
+    """A ragged batch: per tile, nx and ny drawn independently log-uniform in
+    [side_min, side_max], its own generator seed, 0..max_pits pits (radii scaled by
+    max(nx, ny)/1024) and a boundary mode drawn from {normal, periodic_EW}.
+    Returns a list of dicts (z, nx, ny, dx, mode)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(side_min), np.log(side_max)
+    tiles = []
+    for t in range(ntiles):
+        nx = int(round(np.exp(rng.uniform(lo, hi))))
+        ny = int(round(np.exp(rng.uniform(lo, hi))))
+        npits = int(rng.integers(0, max_pits + 1))
+        mode = "periodic_EW" if rng.integers(0, 2) else "normal"
+        z = spectral_dem(nx, ny, seed * 100003 + t, relief=relief, dx=dx, npits=npits,
+                         pit_scale=max(nx, ny) / 1024.0)
+        tiles.append(dict(z=z, nx=nx, ny=ny, dx=dx, mode=mode))
+    return tiles

@@ -194,6 +194,77 @@ int pff_batch_route(const float *z, int32_t *receivers, float *gradient, float *
 int pff_batch_status(long long total_cells, int ntiles, void *workspace, size_t workspace_bytes,
                      int *status, void *stream);
 
+/* GraphFlood on every tile of a planned batch, one persistent launch: each tile runs
+ * Flooder iterations (gf_fields.py:126-141: receivers, carve reroute, fill with
+ * delta 1e-3, 5 diffusion sweeps, Manning update) until its stop or `niter`.
+ * zh (the packed DEMs), h and Q are updated in place, bit-identical to a Flooder
+ * per tile.  tile_consts: 4 floats per tile in caller order -- float(dx^2),
+ * float(prec*dx^2), float(manning), and the stop threshold on the iteration's
+ * change of h; crit 0 stops a tile when max|dh| < threshold (the reference's
+ * max|dh|/dt < tol*prec with threshold = tol*prec*dt), 1 when mean|dh| < threshold,
+ * -1 never.  Per tile (caller order): iters = iterations run, residuals = the last
+ * (max|dh|, mean|dh|); trace (optional): niter x (max, mean) per tile.  The mean is
+ * summed in an unspecified order.  Asynchronous; status bits as pff_batch_status. */
+int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts, float edgesw, float dt,
+                         int niter, int crit, int32_t *iters, float *residuals, float *trace,
+                         long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
+/* ---- Warm-start network (BF16 tensor-core convolutions) ---------------------------
+ * No reference counterpart: the reference has no learned component.  These serve
+ * a U-Net that predicts an initial GraphFlood water depth.  Activations are NHWC
+ * bf16 (uint16_t bits) rows of `cs` channels; an operand is the channel slice
+ * [off, off + C) of its rows.  Weights are [Cout][9][Cin] bf16 (tap = kh*3 + kw).
+ * 3x3 convolutions have stride 1 and zero padding 1; products accumulate in f32.
+ *
+ * pff_conv3x3_fwd: y = conv(x, w) + bias (bias f32, may be NULL), ReLU if relu,
+ *   y stored as bf16 (out_f32 = 0) or f32.  Cin, csx, offx multiples of 8.
+ * pff_conv3x3_wflip: wt[ci][tap][co] = w[co][8 - tap][ci]; the data gradient of a
+ *   convolution is pff_conv3x3_fwd of dy with wt (Cin and Cout exchanged).
+ * pff_conv3x3_wgrad: dw[co][tap*Cin + ci] += sum over pixels of dy * shifted x
+ *   (f32, accumulated atomically: zero dw first).  Channels multiples of 8.
+ * pff_bias_grad: db[c] += sum over pixels of dy[p][c] (C <= 256).
+ * pff_relu_bwd: g = 0 where y <= 0 (y the ReLU output).
+ * pff_avgpool2 / _bwd: 2x2 mean pooling (H, W of the fine grid, both even); the
+ *   backward spreads dy / 4, adding to dx if accumulate.
+ * pff_upsample2 / _bwd: nearest 2x upsampling (H, W of the coarse grid); the
+ *   backward sums each 2x2 block.
+ * pff_mse_loss: loss += scale * sum w (pred - t)^2 over pred channel 0 (rows of csp
+ *   floats; weight may be NULL), dpred rows (csd bf16) = (2 w (pred - t) scale, 0...).
+ * pff_adam: Adam with decoupled weight decay, step >= 1; writes the bf16 copy if
+ *   p_bf16 is not NULL.
+ * pff_unet_features: 8-channel bf16 input rows for B tiles of N cells from the
+ *   elevation, steepest slope, drainage counts, per-tile rainfall and Manning n;
+ *   stats receives each tile's elevation mean and 1/std (2 floats per tile).
+ * pff_unet_h0: h0 = max(exp(pred) - eps, 0); pff_unet_target: log(max(h,0) + eps). */
+int pff_conv3x3_fwd(const uint16_t *x, int csx, int offx, const uint16_t *w, const float *bias, void *y,
+                    int csy, int offy, int B, int H, int W, int Cin, int Cout, int relu, int out_f32,
+                    void *stream);
+int pff_conv3x3_wflip(const uint16_t *w, uint16_t *wt, int Cin, int Cout, void *stream);
+int pff_conv3x3_wgrad(const uint16_t *x, int csx, int offx, const uint16_t *dy, int csd, int offd, float *dw,
+                      int B, int H, int W, int Cin, int Cout, void *stream);
+int pff_bias_grad(const uint16_t *dy, int cs, int off, float *db, long long P, int C, void *stream);
+int pff_relu_bwd(uint16_t *g, int csg, int offg, const uint16_t *y, int csy, int offy, long long P, int C,
+                 void *stream);
+int pff_avgpool2(const uint16_t *x, int csx, int offx, uint16_t *y, int csy, int offy, int B, int H, int W,
+                 int C, void *stream);
+int pff_avgpool2_bwd(const uint16_t *dy, int csd, int offd, uint16_t *dx, int csx, int offx, int B, int H,
+                     int W, int C, int accumulate, void *stream);
+int pff_upsample2(const uint16_t *x, int csx, int offx, uint16_t *y, int csy, int offy, int B, int H, int W,
+                  int C, void *stream);
+int pff_upsample2_bwd(const uint16_t *dy, int csd, int offd, uint16_t *dx, int csx, int offx, int B, int H,
+                      int W, int C, void *stream);
+int pff_mse_loss(const float *pred, int csp, const float *target, const float *weight, long long P,
+                 uint16_t *dpred, int csd, float scale, float *loss, void *stream);
+int pff_adam(float *p, const float *g, float *m, float *v, uint16_t *p_bf16, long long n, float lr, float b1,
+             float b2, float eps, int step, float weight_decay, void *stream);
+int pff_f32_to_bf16(const float *src, uint16_t *dst, long long n, void *stream);
+int pff_unet_features(const float *z, const float *slope, const uint32_t *counts, const float *prec,
+                      const float *manning, float dx, int B, long long N, float *stats, uint16_t *out,
+                      void *stream);
+int pff_unet_h0(const float *pred, int cs, float *h0, long long P, float eps, void *stream);
+int pff_unet_target(const float *h, float *target, long long P, float eps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,23 @@ SIGNATURES = {
     "pff_batch_plan": (_i64, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
     "pff_batch_route": (_i32, [_vp] * 5 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),
     "pff_batch_status": (_i32, [_i64, _i32, _vp, _sz, C.POINTER(C.c_int), _vp]),
+    "pff_batch_graphflood": (_i32, [_vp, _vp, _vp, _vp, _f32, _f32, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32,
+                                    _i32, _vp, _sz, _vp]),
+    "pff_conv3x3_fwd": (_i32, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32] + [_i32] * 7 + [_vp]),
+    "pff_conv3x3_wflip": (_i32, [_vp, _vp, _i32, _i32, _vp]),
+    "pff_conv3x3_wgrad": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32, _vp] + [_i32] * 5 + [_vp]),
+    "pff_bias_grad": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp]),
+    "pff_relu_bwd": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32, _i64, _i32, _vp]),
+    "pff_avgpool2": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32] + [_i32] * 4 + [_vp]),
+    "pff_avgpool2_bwd": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32] + [_i32] * 5 + [_vp]),
+    "pff_upsample2": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32] + [_i32] * 4 + [_vp]),
+    "pff_upsample2_bwd": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32] + [_i32] * 4 + [_vp]),
+    "pff_mse_loss": (_i32, [_vp, _i32, _vp, _vp, _i64, _vp, _i32, _f32, _vp, _vp]),
+    "pff_adam": (_i32, [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _f32, _i32, _f32, _vp]),
+    "pff_f32_to_bf16": (_i32, [_vp, _vp, _i64, _vp]),
+    "pff_unet_features": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _i32, _i64, _vp, _vp, _vp]),
+    "pff_unet_h0": (_i32, [_vp, _i32, _vp, _i64, _f32, _vp]),
+    "pff_unet_target": (_i32, [_vp, _vp, _i64, _f32, _vp]),
 }
 
 _lib = None

@@ -20,7 +20,9 @@ struct BatchTile {
     long long off;   // first cell of the tile in the packed arrays
     long long boff;  // first basin entry (N+1 entries per tile)
     int nx, ny, mode;
+    int id;          // the tile's index in the caller's order
     float dx;
+    int pad;
 };
 
 // Packed per-cell and per-basin arrays of the batch (device pointers).
@@ -476,19 +478,14 @@ __device__ void tile_accumulate(int N, const int32_t *rcv, float *p, uint32_t *c
     __syncthreads();
 }
 
+// receivers (receivers.py:31-58): strict >, first k wins ties.  Writes rec and rec_
+// (and the gradient if grad is not null).
 template <int MODE>
-__device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &sh)
+__device__ void tile_receivers(const Grid &g, float dx, const float *z, int32_t *rec, int32_t *rec_, float *grad)
 {
-    const Grid g{T.nx, T.ny, MODE, nullptr};
-    const int N = T.nx * T.ny;
-    const long long o = T.off, ob = T.boff;
-    const float *z = A.z + o;
-    int32_t *rec = A.rcv + o, *rec_ = A.rec_ + o, *rec__ = A.rec__ + o, *bid = A.bid + o;
-    const int lrounds = bceil_log2(N) + 1;
-
-    // receivers (receivers.py:31-58): strict >, first k wins ties
+    const int N = g.nx * g.ny;
     FOR_CELLS(i, N) {
-        const int row = i / T.nx, col = i - row * T.nx;
+        const int row = i / g.nx, col = i - row * g.nx;
         int js[4];
         neighbours4<MODE>(g, i, row, col, js);
         const float zi = z[i];
@@ -499,7 +496,7 @@ __device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &s
             if (js[k] == -1) continue;
             const float d = __fsub_rn(zi, z[js[k]]);
             if (d > dbest) {  // a smaller difference cannot give a larger quotient
-                const float q = __fdiv_rn(d, T.dx);
+                const float q = __fdiv_rn(d, dx);
                 if (q > sr) {
                     sr = q;
                     r = js[k];
@@ -509,32 +506,233 @@ __device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &s
         }
         rec[i] = r;
         rec_[i] = r;
-        A.grad[o + i] = sr;
+        if (grad) grad[i] = sr;
     }
     __syncthreads();
+}
 
-    // reroute_flow(carve=True) (lakeflow.py:466-538)
+// reroute_flow(carve=True) (lakeflow.py:466-538) on receivers rec (with rec_ == rec).
+template <int MODE>
+__device__ void tile_reroute(const Grid &g, const BatchTile &T, const BatchArrays &A, const float *z, BatchShm &sh)
+{
+    const int N = g.nx * g.ny;
+    const long long o = T.off, ob = T.boff;
+    int32_t *rec = A.rcv + o, *rec_ = A.rec_ + o, *rec__ = A.rec__ + o, *bid = A.bid + o;
+    const int lrounds = bceil_log2(N) + 1;
     int np = 0;
     FOR_CELLS(i, N) np += (rec_[i] == i && !leave<MODE>(g, i));
     const int ndep = bsum(np, sh);
-    if (ndep > 0) {
-        const int outer = bceil_log2(ndep) + 1;
-        for (int it = 0; it < outer; ++it) {
-            int nb = 0;
-            if (it > 0) FOR_CELLS(i, N) nb += (rec_[i] == i && !leave<MODE>(g, i));
-            const int nd = it > 0 ? bsum(nb, sh) : ndep;
-            if (nd == 0) break;  // (the labels the reference computes first are overwritten)
-            tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
-            tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
-                                  A.inv + ob, z);
-            tile_carve(N, rec, rec_, rec__, A.mark + o, A.tag + o, A.tag_ + o, A.snode + ob, A.outlet + ob,
-                       A.status);
-        }
+    if (ndep == 0) return;
+    const int outer = bceil_log2(ndep) + 1;
+    for (int it = 0; it < outer; ++it) {
+        int nb = 0;
+        if (it > 0) FOR_CELLS(i, N) nb += (rec_[i] == i && !leave<MODE>(g, i));
+        const int nd = it > 0 ? bsum(nb, sh) : ndep;
+        if (nd == 0) break;  // (the labels the reference computes first are overwritten)
+        tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
+        tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
+                              A.inv + ob, z);
+        tile_carve(N, rec, rec_, rec__, A.mark + o, A.tag + o, A.tag_ + o, A.snode + ob, A.outlet + ob, A.status);
     }
+}
 
+template <int MODE>
+__device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &sh)
+{
+    const Grid g{T.nx, T.ny, MODE, nullptr};
+    const int N = T.nx * T.ny;
+    const long long o = T.off;
+    const float *z = A.z + o;
+    tile_receivers<MODE>(g, T.dx, z, A.rcv + o, A.rec_ + o, A.grad + o);
+    tile_reroute<MODE>(g, T, A, z, sh);
     // accumulate: Q holds the seed (flowfields.py:272-292)
-    tile_accumulate(N, rec, A.Q + o, A.counts + o, A.dnr + 4 * o, A.dnr_ + 4 * o, A.ndnr + o, A.ndnr_ + o, A.src + o,
-                    A.p_ + o, A.c_ + o);
+    tile_accumulate(N, A.rcv + o, A.Q + o, A.counts + o, A.dnr + 4 * o, A.dnr_ + 4 * o, A.ndnr + o, A.ndnr_ + o,
+                    A.src + o, A.p_ + o, A.c_ + o);
+}
+
+// ---- GraphFlood on a tile (gf_fields.py:126-141) --------------------------------------
+//
+// One iteration: receivers, carve reroute, fill with delta (fill_topo.py:17-45,
+// snapshot rounds), 5 diffusion sweeps (gf_hydrodynamics.py:24-75, sums in the
+// serial order), Manning update (gf_hydrodynamics.py:79-129).  Per-tile constants
+// are the f32 values the single-grid Flooder passes: dx2, prec*dx^2, manning.
+struct GfParams {
+    const float *cst;  // per tile (caller order): dx2, prec_dx2, manning, stop threshold on max|dh|
+    float edgesw, dt, eps;
+    int niter;
+    int crit;          // 0: stop when max|dh| < threshold; 1: when mean|dh| < threshold; -1: never
+    float *h;          // packed, in/out
+    int32_t *iters;    // per tile (caller order): iterations run
+    float *res;        // per tile: last max|dh| and mean|dh| (2 floats)
+    float *trace;      // optional, per tile: niter x (max|dh|, mean|dh|)
+};
+
+// max and sum of v over the block (max as unsigned bits: |x| >= 0, NaN above all)
+__device__ __forceinline__ void bmaxsum(float m, float sum, BatchShm &sh, float *om, float *os)
+{
+    unsigned mu = __float_as_uint(m);
+    for (int o = 16; o; o >>= 1) {
+        mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { sh.ws[0] = 0; sh.ws[1] = 0; }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax((unsigned *)&sh.ws[0], mu);
+        atomicAdd((float *)&sh.ws[1], sum);
+    }
+    __syncthreads();
+    *om = __uint_as_float((unsigned)sh.ws[0]);
+    *os = __int_as_float(sh.ws[1]);
+    __syncthreads();
+}
+
+template <int MODE>
+__device__ void gf_tile(const BatchTile &T, const BatchArrays &A, const GfParams &P, BatchShm &sh)
+{
+    const Grid g{T.nx, T.ny, MODE, nullptr};
+    const int N = T.nx * T.ny;
+    const long long o = T.off;
+    float *zh = const_cast<float *>(A.z) + o, *h = P.h + o, *Q = A.Q + o;
+    int32_t *rec = A.rcv + o;
+    // scratch of the routing arrays, free once the reroute is done
+    int32_t *ra = A.rec_ + o, *rb = A.rec__ + o;
+    float *zs = A.zp + o, *zn = A.p_ + o;
+    float *w = reinterpret_cast<float *>(A.dnr_) + 4 * o;
+    uint8_t *issrc = A.isb + o;
+    float *temp = reinterpret_cast<float *>(A.ndnr) + o;
+    float *href = reinterpret_cast<float *>(A.c_) + o;
+    float *dh = reinterpret_cast<float *>(A.ndnr_) + o;
+    const float dx = T.dx, dx2 = P.cst[4 * T.id], prec_dx2 = P.cst[4 * T.id + 1], manning = P.cst[4 * T.id + 2];
+    const float thr = P.cst[4 * T.id + 3];
+    const int nr = bceil_log2(N);
+    int it = 0;
+    float rmax = 0.f, rmean = 0.f;
+    for (; it < P.niter; ++it) {
+        FOR_CELLS(i, N) href[i] = h[i];
+        tile_receivers<MODE>(g, dx, zh, rec, A.rec_ + o, nullptr);
+        tile_reroute<MODE>(g, T, A, zh, sh);
+        // fill_z_add_delta (fill_topo.py:99-125): rounds on snapshots of z_ and rec_
+        FOR_CELLS(i, N) {
+            zs[i] = zh[i];
+            ra[i] = rec[i];
+        }
+        __syncthreads();
+        float *a = zs, *b = zn;
+        int32_t *pa = ra, *pb = rb;
+        for (int r = 0; r < nr; ++r) {
+            const float inc = (float)(ldexp(1.0, r - 1) * (double)P.eps);
+            FOR_CELLS(i, N) {
+                const int q = pa[i];
+                const int qq = pa[q];
+                pb[i] = qq;
+                const float zi = a[i];
+                if (i == q || (zi > zh[q] && qq == q)) b[i] = zi;
+                else b[i] = fmaxf(zi, __fadd_rn(a[q], inc));
+            }
+            __syncthreads();
+            float *t = a; a = b; b = t;
+            int32_t *u = pa; pa = pb; pb = u;
+        }
+        FOR_CELLS(i, N) {
+            const float zf = a[i];
+            h[i] = __fadd_rn(h[i], __fsub_rn(zf, zh[i]));
+            zh[i] = zf;
+        }
+        __syncthreads();
+        // diffusion: weights once, then 5 gather sweeps (Q <-> temp), ending in Q
+        FOR_CELLS(i, N) {
+            const int row = i / g.nx, col = i - row * g.nx;
+            if (leave<MODE>(g, i)) { issrc[i] = 0; continue; }
+            const float zi = zh[i];
+            float sk[4];
+            float sums = 0.f;
+            int js[4];
+            neighbours4<MODE>(g, i, row, col, js);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                sk[k] = (js[k] != -1) ? fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zh[js[k]]), dx)) : 0.f;
+                sums = __fadd_rn(sums, sk[k]);
+            }
+            if (sums == 0.f) { issrc[i] = 0; continue; }
+            issrc[i] = 1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) w[(size_t)k * N + i] = __fdiv_rn(sk[k], sums);
+        }
+        __syncthreads();
+        float *qa = Q, *qb = temp;
+        for (int sw = 0; sw < 5; ++sw) {
+            FOR_CELLS(j, N) {
+                const int row = j / g.nx, col = j - row * g.nx;
+                float acc = prec_dx2;
+                if (row > 0 && row < g.ny - 1 && col > 0 && col < g.nx - 1) {
+                    const int nx = g.nx;
+                    if (issrc[j - nx]) acc = __fadd_rn(acc, __fmul_rn(w[3 * (size_t)N + j - nx], qa[j - nx]));
+                    if (issrc[j - 1]) acc = __fadd_rn(acc, __fmul_rn(w[2 * (size_t)N + j - 1], qa[j - 1]));
+                    if (issrc[j + 1]) acc = __fadd_rn(acc, __fmul_rn(w[(size_t)N + j + 1], qa[j + 1]));
+                    if (issrc[j + nx]) acc = __fadd_rn(acc, __fmul_rn(w[j + nx], qa[j + nx]));
+                } else {
+                    int c[8];
+                    const int n = donor_candidates(g, j, row, col, c);
+                    for (int q = 0; q < n; ++q) {
+                        const int i = c[q];
+                        if (!issrc[i]) continue;
+                        const float qi = qa[i];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (neighbour_i<MODE>(g, i, k) == j) acc = __fadd_rn(acc, __fmul_rn(w[(size_t)k * N + i], qi));
+                    }
+                }
+                qb[j] = acc;
+            }
+            __syncthreads();
+            float *t = qa; qa = qb; qb = t;
+        }
+        if (qa != Q) {
+            FOR_CELLS(j, N) Q[j] = qa[j];
+            __syncthreads();
+        }
+        // Manning update, two loops as in the reference (h receives tdh twice)
+        FOR_CELLS(i, N) {
+            const int r = rec[i];
+            float tS = P.edgesw;
+            if (r != i) tS = fmaxf(__fdiv_rn(__fsub_rn(zh[i], zh[r]), dx), 1e-4f);
+            float Qo = __fmul_rn(dx, (float)pow((double)h[i], (double)(5.0f / 3.0f)));
+            Qo = __fdiv_rn(Qo, manning);
+            Qo = __fmul_rn(Qo, __fsqrt_rn(tS));
+            float tdh = __fdiv_rn(__fsub_rn(Q[i], Qo), dx2);
+            tdh = __fmul_rn(tdh, P.dt);
+            const float h1 = __fadd_rn(h[i], tdh);
+            h[i] = h1;
+            if (h1 < 0.f) tdh = __fadd_rn(tdh, h1);
+            dh[i] = tdh;
+        }
+        __syncthreads();
+        float m = 0.f, sum = 0.f;
+        FOR_CELLS(i, N) {
+            const float d = dh[i];
+            const float hn = __fadd_rn(h[i], d);
+            h[i] = hn;
+            zh[i] = __fadd_rn(zh[i], d);
+            const float e = fabsf(__fsub_rn(hn, href[i]));
+            m = __uint_as_float(max(__float_as_uint(m), __float_as_uint(e)));
+            sum += e;
+        }
+        bmaxsum(m, sum, sh, &rmax, &rmean);
+        rmean /= (float)N;
+        if (P.trace && threadIdx.x == 0) {
+            P.trace[((size_t)T.id * P.niter + it) * 2] = rmax;
+            P.trace[((size_t)T.id * P.niter + it) * 2 + 1] = rmean;
+        }
+        if ((P.crit == 0 && rmax < thr) || (P.crit == 1 && rmean < thr)) { ++it; break; }
+    }
+    if (threadIdx.x == 0) {
+        P.iters[T.id] = it;
+        P.res[2 * T.id] = rmax;
+        P.res[2 * T.id + 1] = rmean;
+    }
+    __syncthreads();
 }
 
 // Persistent: each CTA takes the next tile (largest first) until the queue is empty.
@@ -552,6 +750,29 @@ __global__ void __launch_bounds__(1024) k_batch_route(int ntiles, BatchArrays A)
         case 0: route_tile<0>(T, A, sh); break;
         case 1: route_tile<1>(T, A, sh); break;
         case 2: route_tile<2>(T, A, sh); break;
+        default:
+            if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
+            break;
+        }
+        __syncthreads();
+    }
+}
+
+// Persistent GraphFlood: each CTA runs whole tiles to their stop, largest first.
+__global__ void __launch_bounds__(1024) k_batch_graphflood(int ntiles, BatchArrays A, GfParams P)
+{
+    __shared__ BatchShm sh;
+    for (;;) {
+        if (threadIdx.x == 0) sh.cur = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int k = sh.cur;
+        __syncthreads();
+        if (k >= ntiles) return;
+        const BatchTile T = A.tiles[k];
+        switch (T.mode) {
+        case 0: gf_tile<0>(T, A, P, sh); break;
+        case 1: gf_tile<1>(T, A, P, sh); break;
+        case 2: gf_tile<2>(T, A, P, sh); break;
         default:
             if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
             break;
@@ -669,7 +890,7 @@ extern "C" long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_
     BatchTile *ht = new BatchTile[ntiles];
     for (int k = 0; k < ntiles; ++k) {
         const int t = ord[k];
-        ht[k] = BatchTile{tile_offset[t], tile_offset[t] + t, tile_nx[t], tile_ny[t], tile_mode[t], tile_dx[t]};
+        ht[k] = BatchTile{tile_offset[t], tile_offset[t] + t, tile_nx[t], tile_ny[t], tile_mode[t], t, tile_dx[t], 0};
         if (order) order[k] = t;
     }
     BatchWs w = carve_batch(workspace, workspace_bytes, total, ntiles);
@@ -733,4 +954,40 @@ extern "C" int pff_batch_status(long long total_cells, int ntiles, void *workspa
     PFF_CUDA(cudaMemcpyAsync(status, w.A.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     PFF_CUDA(cudaStreamSynchronize(st));
     return PFF_OK;
+}
+
+extern "C" int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts, float edgesw, float dt,
+                                    int niter, int crit, int32_t *iters, float *residuals, float *trace,
+                                    long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
+                                    size_t workspace_bytes, void *stream)
+{
+    clear_error();
+    PFF_TRY(batch_check(total_cells, ntiles, workspace, workspace_bytes, "pff_batch_graphflood"));
+    if (!zh || !h || !Q || !tile_consts || !iters || !residuals || niter < 0 || crit < -1 || crit > 1) {
+        set_error("pff_batch_graphflood: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    if (threads != 256 && threads != 512 && threads != 1024) {
+        set_error("pff_batch_graphflood: threads must be 256, 512 or 1024 (got %d)", threads);
+        return PFF_ERR_ARG;
+    }
+    int dev = 0, nsm = 148, occ = 1;
+    PFF_CUDA(cudaGetDevice(&dev));
+    PFF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PFF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_graphflood, threads, 0));
+    if (ctas_per_sm < 1) ctas_per_sm = 1;
+    if (ctas_per_sm > occ) ctas_per_sm = occ > 0 ? occ : 1;
+    BatchWs w = carve_batch(workspace, workspace_bytes, total_cells, ntiles);
+    BatchArrays A = w.A;
+    A.z = zh;
+    A.Q = Q;
+    A.rcv = A.src;  // the rerouted receivers of each iteration (the accumulation arrays are unused)
+    A.grad = nullptr;
+    A.counts = nullptr;
+    GfParams P{tile_consts, edgesw, dt, 1e-3f, niter, crit, h, iters, residuals, trace};
+    cudaStream_t st = S(stream);
+    const int grid = std::min(nsm * ctas_per_sm, ntiles);
+    { k_batch_reset<<<1, 1, 0, st>>>(w.ctr); count_launch(); }
+    { k_batch_graphflood<<<grid, threads, 0, st>>>(ntiles, A, P); count_launch(); }
+    return check_cuda("pff_batch_graphflood");
 }

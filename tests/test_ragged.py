@@ -34,7 +34,11 @@ def oracle_chain(orc, t, seed):
 
 
 def bits(a):
-    return np.ascontiguousarray(a, np.float32).view(np.uint32).ravel()
+    """f32 bit patterns, every NaN mapped to one pattern (positions compared, payloads not)."""
+    a = np.ascontiguousarray(a, np.float32).ravel()
+    b = a.view(np.uint32).copy()
+    b[np.isnan(a)] = 0x7FC00000
+    return b
 
 
 def _plan(lib, nx, ny, mode, dx, ws=None, wsb=0):
@@ -148,3 +152,53 @@ def test_ragged_matches_flowrouter(cuda):
         assert np.array_equal(rr.get_receivers(k).ravel(), fr.get_receivers().ravel())
         assert np.array_equal(rr.get_counts(k), fr.get_counts())
         assert np.array_equal(bits(rr.get_Q(k)), bits(fr.get_Q()))
+
+
+@pytest.mark.gpu
+def test_ragged_graphflood_bit_exact_vs_oracle(orc, cuda):
+    """GraphFlood on every tile in one launch equals the reference iteration
+    (oracle, f32) run on each tile alone, with per-tile rainfall and Manning n."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+
+    tiles = synthetic.ragged_tiles(ntiles=6, seed=31, side_min=24, side_max=72, max_pits=8, dx=10.0)
+    tiles[2]["mode"] = "periodic_NS"
+    rr = pf.flow.RaggedRouter([(t["ny"], t["nx"]) for t in tiles], 10.0, [t["mode"] for t in tiles])
+    rr.set_z([t["z"] for t in tiles])
+    P = [1e-5 * (1 + k) for k in range(len(tiles))]
+    n = [0.02 + 0.008 * k for k in range(len(tiles))]
+    fl = pf.graphflood.RaggedFlooder(rr, precipitation_rates=P, manning=n)
+    niter = 40
+    it, res, tr = fl.run(niter, stop=None, trace=True)
+    torch.cuda.synchronize()
+    assert (it == niter).all()
+    for k, t in enumerate(tiles):
+        g = orc.Grid(t["nx"], t["ny"], MODES[t["mode"]])
+        zh = t["z"].ravel().copy()
+        h = np.zeros_like(zh)
+        Q = np.zeros_like(zh)
+        otr = orc.graphflood_run(zh, h, Q, g, 10.0, P[k], manning=n[k], niter=niter)
+        o, N = int(rr.offset[k]), rr.cells(k)
+        assert np.array_equal(bits(fl.get_h(k)), bits(h)), f"tile {k} h"
+        assert np.array_equal(bits(rr.z[o:o + N].cpu().numpy()), bits(zh)), f"tile {k} z"
+        assert np.array_equal(bits(rr.Q[o:o + N].cpu().numpy()), bits(Q)), f"tile {k} Q"
+        assert np.array_equal(bits(tr[k, :, 0]), bits(otr)), f"tile {k} residual trace"
+
+
+@pytest.mark.gpu
+def test_ragged_graphflood_stops_per_tile(cuda):
+    torch = cuda
+    import pyfastflow_b200 as pf
+
+    tiles = synthetic.ragged_tiles(ntiles=4, seed=32, side_min=24, side_max=48, max_pits=3, dx=10.0)
+    rr = pf.flow.RaggedRouter([(t["ny"], t["nx"]) for t in tiles], 10.0, [t["mode"] for t in tiles])
+    rr.set_z([t["z"] for t in tiles])
+    fl = pf.graphflood.RaggedFlooder(rr, precipitation_rates=1e-5)
+    it, res, tr = fl.run(300, stop="mean", tol_ratio=1e4, trace=True)
+    for k in range(len(tiles)):
+        n = int(it[k])
+        assert 1 <= n <= 300
+        if n < 300:  # stopped on its own criterion, at the first iteration below the threshold
+            thr = np.float32(1e4 * 1e-5 * 5e-3)
+            assert tr[k, n - 1, 1] < thr and (tr[k, :n - 1, 1] >= thr).all()
+        assert bits(res[k, 0]) == bits(tr[k, n - 1, 0])  # (a tile whose h went NaN never stops early)

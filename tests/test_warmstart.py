@@ -1,0 +1,259 @@
+"""Warm-start network kernels against PyTorch CPU in float32 (the reference for
+these floating-point kernels): BF16 tensor-core 3x3 convolution forward, data and
+weight gradients, pooling, upsampling, loss, Adam, and the whole U-Net's
+parameter gradients.  Inputs are rounded to bf16 first, so the CPU side sees the
+same operands; tolerances cover bf16 rounding of the outputs and f32 summation
+order."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+F = torch.nn.functional
+
+
+def _bf(t):
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def _nhwc(t):  # NCHW -> flat NHWC
+    return t.permute(0, 2, 3, 1).contiguous().reshape(-1)
+
+
+def _nchw(flat, B, H, W, C):
+    return flat.reshape(B, H, W, C).permute(0, 3, 1, 2)
+
+
+def _w_ours(w):  # [Cout][Cin][3][3] -> [Cout][9][Cin]
+    return w.permute(0, 2, 3, 1).contiguous().reshape(-1)
+
+
+def _rel(a, b):
+    return float((a - b).abs().max() / (b.abs().max() + 1e-12))
+
+
+def test_unet_layer_table_consistent():
+    from pyfastflow_b200.warmstart.unet import BUFFERS, LAYERS
+
+    for name, src, so, dst, do, cin, cout, relu, lev in LAYERS:
+        assert so + cin <= BUFFERS[src][0] and do + cout <= BUFFERS[dst][0], name
+        assert BUFFERS[src][1] == lev and BUFFERS[dst][1] == lev, name
+        assert cin % 8 == 0 and cout % 8 == 0, name
+    assert max(L[6] for L in LAYERS) == 256 and LAYERS[0][6] == 32
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,H,W,Cin,Cout,relu", [(2, 10, 12, 16, 24, 1), (1, 33, 7, 8, 64, 0), (3, 16, 16, 96, 72, 1)])
+def test_conv_forward(cuda, B, H, W, Cin, Cout, relu):
+    from pyfastflow_b200 import _dev, _lib
+
+    g = torch.Generator().manual_seed(B * 100 + Cin)
+    x = _bf(torch.randn(B, Cin, H, W, generator=g))
+    w = _bf(torch.randn(Cout, Cin, 3, 3, generator=g) * 0.2)
+    b = torch.randn(Cout, generator=g)
+    ref = F.conv2d(x, w, b, padding=1)
+    if relu:
+        ref = ref.clamp_min(0)
+    xd = _nhwc(x).to(torch.bfloat16).cuda()
+    wd = _w_ours(w).to(torch.bfloat16).cuda()
+    bd = b.cuda()
+    y32 = torch.zeros(B * H * W * Cout, dtype=torch.float32, device="cuda")
+    _lib.call("pff_conv3x3_fwd", xd.data_ptr(), Cin, 0, wd.data_ptr(), bd.data_ptr(), y32.data_ptr(), Cout, 0, B, H,
+              W, Cin, Cout, relu, 1, _dev.stream())
+    out = _nchw(y32.cpu(), B, H, W, Cout)
+    assert _rel(out, ref) < 2e-5 * np.sqrt(9 * Cin) + 1e-5
+    y16 = torch.zeros(B * H * W * Cout, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_conv3x3_fwd", xd.data_ptr(), Cin, 0, wd.data_ptr(), bd.data_ptr(), y16.data_ptr(), Cout, 0, B, H,
+              W, Cin, Cout, relu, 0, _dev.stream())
+    assert _rel(_nchw(y16.float().cpu(), B, H, W, Cout), ref) < 1e-2
+
+
+@pytest.mark.gpu
+def test_conv_channel_slices(cuda):
+    """Input read from channels [8, 24) of 32-channel rows, output written to
+    channels [16, 40) of 48-channel rows; the rest of the output rows untouched."""
+    from pyfastflow_b200 import _dev, _lib
+
+    B, H, W, Cin, Cout = 2, 9, 11, 16, 24
+    g = torch.Generator().manual_seed(5)
+    xw = _bf(torch.randn(B, 32, H, W, generator=g))
+    w = _bf(torch.randn(Cout, Cin, 3, 3, generator=g) * 0.2)
+    ref = F.conv2d(xw[:, 8:24], w, padding=1)
+    xd = _nhwc(xw).to(torch.bfloat16).cuda()
+    y = torch.full((B * H * W * 48,), 7.0, dtype=torch.float32, device="cuda")
+    _lib.call("pff_conv3x3_fwd", xd.data_ptr(), 32, 8, _w_ours(w).to(torch.bfloat16).cuda().data_ptr(), None,
+              y.data_ptr(), 48, 16, B, H, W, Cin, Cout, 0, 1, _dev.stream())
+    yy = _nchw(y.cpu(), B, H, W, 48)
+    assert _rel(yy[:, 16:40], ref) < 1e-4
+    assert (yy[:, :16] == 7).all() and (yy[:, 40:] == 7).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("B,H,W,Cin,Cout", [(2, 12, 10, 16, 32), (1, 40, 24, 64, 8), (2, 8, 8, 32, 128)])
+def test_conv_gradients(cuda, B, H, W, Cin, Cout):
+    """Data gradient (forward kernel on flipped weights), weight and bias
+    gradients against torch autograd."""
+    from pyfastflow_b200 import _dev, _lib
+
+    g = torch.Generator().manual_seed(H * W + Cout)
+    x = _bf(torch.randn(B, Cin, H, W, generator=g)).requires_grad_(True)
+    w = _bf(torch.randn(Cout, Cin, 3, 3, generator=g) * 0.2).requires_grad_(True)
+    b = torch.zeros(Cout, requires_grad=True)
+    dy = _bf(torch.randn(B, Cout, H, W, generator=g))
+    F.conv2d(x, w, b, padding=1).backward(dy)
+    st = _dev.stream()
+    wd = _w_ours(w.detach()).to(torch.bfloat16).cuda()
+    wt = torch.zeros_like(wd)
+    _lib.call("pff_conv3x3_wflip", wd.data_ptr(), wt.data_ptr(), Cin, Cout, st)
+    dyd = _nhwc(dy).to(torch.bfloat16).cuda()
+    dx = torch.zeros(B * H * W * Cin, dtype=torch.float32, device="cuda")
+    _lib.call("pff_conv3x3_fwd", dyd.data_ptr(), Cout, 0, wt.data_ptr(), None, dx.data_ptr(), Cin, 0, B, H, W, Cout,
+              Cin, 0, 1, st)
+    assert _rel(_nchw(dx.cpu(), B, H, W, Cin), x.grad) < 1e-4
+    xd = _nhwc(x.detach()).to(torch.bfloat16).cuda()
+    dw = torch.zeros(Cout * 9 * Cin, dtype=torch.float32, device="cuda")
+    _lib.call("pff_conv3x3_wgrad", xd.data_ptr(), Cin, 0, dyd.data_ptr(), Cout, 0, dw.data_ptr(), B, H, W, Cin, Cout,
+              st)
+    dw_ref = _w_ours(w.grad)
+    assert _rel(dw.cpu(), dw_ref) < 1e-4
+    db = torch.zeros(Cout, dtype=torch.float32, device="cuda")
+    _lib.call("pff_bias_grad", dyd.data_ptr(), Cout, 0, db.data_ptr(), B * H * W, Cout, st)
+    assert _rel(db.cpu(), b.grad) < 1e-4
+
+
+@pytest.mark.gpu
+def test_pool_upsample_relu(cuda):
+    from pyfastflow_b200 import _dev, _lib
+
+    B, H, W, C = 2, 8, 12, 16
+    st = _dev.stream()
+    g = torch.Generator().manual_seed(9)
+    x = _bf(torch.randn(B, C, H, W, generator=g))
+    xd = _nhwc(x).to(torch.bfloat16).cuda()
+    y = torch.zeros(B * H * W * C // 4, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_avgpool2", xd.data_ptr(), C, 0, y.data_ptr(), C, 0, B, H, W, C, st)
+    assert _rel(_nchw(y.float().cpu(), B, H // 2, W // 2, C), F.avg_pool2d(x, 2)) < 1e-2
+    # pooling backward adds into a slice of wider rows
+    dy = _bf(torch.randn(B, C, H // 2, W // 2, generator=g))
+    base = torch.ones(B * H * W * 2 * C, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_avgpool2_bwd", _nhwc(dy).to(torch.bfloat16).cuda().data_ptr(), C, 0, base.data_ptr(), 2 * C, C, B,
+              H, W, C, 1, st)
+    got = _nchw(base.float().cpu(), B, H, W, 2 * C)
+    ref = 1 + F.interpolate(dy, scale_factor=2, mode="nearest") / 4
+    assert _rel(got[:, C:], ref) < 1e-2 and (got[:, :C] == 1).all()
+    # upsampling into the first channels of concatenation rows, and its backward
+    up = torch.zeros(B * 4 * H * W * 2 * C, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_upsample2", xd.data_ptr(), C, 0, up.data_ptr(), 2 * C, 0, B, H, W, C, st)
+    assert torch.equal(_nchw(up.float().cpu(), B, 2 * H, 2 * W, 2 * C)[:, :C],
+                       F.interpolate(x, scale_factor=2, mode="nearest"))
+    du = _bf(torch.randn(B, 2 * C, 2 * H, 2 * W, generator=g))
+    dxu = torch.zeros(B * H * W * C, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_upsample2_bwd", _nhwc(du).to(torch.bfloat16).cuda().data_ptr(), 2 * C, 0, dxu.data_ptr(), C, 0, B,
+              H, W, C, st)
+    assert _rel(_nchw(dxu.float().cpu(), B, H, W, C), F.avg_pool2d(du[:, :C], 2) * 4) < 1e-2
+    # ReLU backward: zero where the output is not positive
+    gr = torch.ones(B * H * W * C, dtype=torch.bfloat16, device="cuda")
+    _lib.call("pff_relu_bwd", gr.data_ptr(), C, 0, xd.data_ptr(), C, 0, B * H * W, C, st)
+    assert torch.equal(gr.float().cpu() > 0, _nhwc(x) > 0)
+
+
+@pytest.mark.gpu
+def test_adam_matches_formula(cuda):
+    from pyfastflow_b200 import _dev, _lib
+
+    n = 1000
+    g = torch.Generator().manual_seed(3)
+    p0, gr = torch.randn(n, generator=g), torch.randn(n, generator=g)
+    p, m, v = p0.clone().cuda(), torch.zeros(n).cuda(), torch.zeros(n).cuda()
+    pb = torch.zeros(n, dtype=torch.bfloat16, device="cuda")
+    for step in (1, 2):
+        _lib.call("pff_adam", p.data_ptr(), gr.cuda().data_ptr(), m.data_ptr(), v.data_ptr(), pb.data_ptr(), n, 1e-2,
+                  0.9, 0.999, 1e-8, step, 0.0, _dev.stream())
+    opt = torch.optim.Adam([p0.requires_grad_(True)], lr=1e-2)
+    for _ in range(2):
+        opt.zero_grad()
+        p0.grad = gr.clone()
+        opt.step()
+    assert torch.allclose(p.cpu(), p0.detach(), rtol=1e-5, atol=1e-6)
+    assert torch.equal(pb.cpu(), p.cpu().to(torch.bfloat16))
+
+
+def _torch_unet(net, x, B, H, W):
+    """The same network in float32 on the CPU, weights rounded to bf16 as ours."""
+    from pyfastflow_b200.warmstart.unet import LAYERS
+
+    p = net.p.cpu()
+    Ws, bs = {}, {}
+    for name, _, _, _, _, cin, cout, _, _ in LAYERS:
+        wo, nw, bo, _ = net.layers[name]
+        Ws[name] = _bf(p[wo:wo + nw]).reshape(cout, 3, 3, cin).permute(0, 3, 1, 2).clone().requires_grad_(True)
+        bs[name] = p[bo:bo + cout].clone().requires_grad_(True)
+    c = lambda n, t, r=True: (F.conv2d(t, Ws[n], bs[n], padding=1).clamp_min(0) if r  # noqa: E731
+                              else F.conv2d(t, Ws[n], bs[n], padding=1))
+    up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")  # noqa: E731
+    e0 = c("enc0b", c("enc0a", x))
+    e1 = c("enc1b", c("enc1a", F.avg_pool2d(e0, 2)))
+    e2 = c("enc2b", c("enc2a", F.avg_pool2d(e1, 2)))
+    e3 = c("botb", c("bota", F.avg_pool2d(e2, 2)))
+    d2 = c("dec2b", c("dec2a", torch.cat([up(e3), e2], 1)))
+    d1 = c("dec1b", c("dec1a", torch.cat([up(d2), e1], 1)))
+    d0 = c("dec0b", c("dec0a", torch.cat([up(d1), e0], 1)))
+    return c("head", d0, False), Ws, bs
+
+
+@pytest.mark.gpu
+def test_unet_gradients_vs_torch(cuda):
+    """Forward prediction and every layer's weight gradient of the whole U-Net
+    (bf16 activations on the GPU) against the f32 CPU network on the same weights."""
+    from pyfastflow_b200 import _dev
+    from pyfastflow_b200.warmstart import UNet
+
+    B, H, W = 2, 16, 24
+    net = UNet(seed=1)
+    net.set_head_bias(0.0)
+    g = torch.Generator().manual_seed(11)
+    x = _bf(torch.randn(B, 8, H, W, generator=g) * 0.5)
+    x[:, 6:] = 0
+    tgt = torch.randn(B * H * W, generator=g)
+    pred = net.forward(_nhwc(x).to(torch.bfloat16).cuda(), B, H, W)
+    loss, dp = net.loss_grad(tgt.cuda())
+    net.backward(dp)
+    torch.cuda.synchronize()
+    ref, Ws, bs = _torch_unet(net, x, B, H, W)
+    pr = ref.permute(0, 2, 3, 1).reshape(-1, 8)[:, 0]
+    ours = pred.cpu().reshape(-1, 8)[:, 0]
+    assert _rel(ours, pr) < 0.03
+    lref = ((pr - tgt) ** 2).mean()
+    assert abs(float(loss) - float(lref)) / float(lref) < 0.02
+    lref.backward()
+    gpu_g = net.g.cpu()
+    for name in Ws:
+        wo, nw, bo, cout = net.layers[name]
+        gw = gpu_g[wo:wo + nw]
+        rw = _w_ours(Ws[name].grad)
+        cos = float(torch.dot(gw, rw) / (gw.norm() * rw.norm() + 1e-30))
+        assert cos > 0.97, f"{name}: cosine {cos:.4f}"
+        assert abs(float(gw.norm() / rw.norm()) - 1) < 0.05, name
+
+
+@pytest.mark.gpu
+def test_unet_training_reduces_loss(cuda):
+    """A few Adam steps on a fixed batch reduce the loss (end-to-end smoke of the
+    training loop on the GPU kernels)."""
+    from pyfastflow_b200.warmstart import UNet
+
+    B, H, W = 4, 32, 32
+    net = UNet(seed=2)
+    g = torch.Generator().manual_seed(12)
+    x = torch.randn(B, H, W, 8, generator=g) * 0.5
+    x[..., 6:] = 0
+    tgt = (2.0 * x[..., 0] + 0.5).reshape(-1).cuda()  # a target the inputs determine
+    xd = x.reshape(-1).to(torch.bfloat16).cuda()
+    losses = []
+    for _ in range(80):
+        net.forward(xd, B, H, W)
+        loss, dp = net.loss_grad(tgt)
+        net.backward(dp)
+        net.adam_step(lr=2e-3)
+        losses.append(float(loss))
+    assert np.isfinite(losses).all()
+    assert losses[-1] < 0.6 * losses[0]

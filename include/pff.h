@@ -164,6 +164,12 @@ int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, cons
                         float dx, float dx2, float manning, float edgesw, float dt,
                         const float *h_ref, float *dhmax, void *stream);
 
+/* out[0] = max |a - b| (maxed into its current value as unsigned bits, so a NaN
+ * difference wins), out[1] += sum |a - b| (f32, unspecified order).  Zero out first.
+ * Used for GraphFlood's residuals (the change of h over an iteration).  No
+ * reference counterpart. */
+int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *stream);
+
 /* ---- Ragged batch ----------------------------------------------------------------
  * Many independent tiles (own nx, ny, dx, boundary mode 0-2) packed back to back,
  * tile t's cells at [tile_offset[t], tile_offset[t] + nx*ny) in row-major order.
@@ -236,7 +242,8 @@ int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts
  * pff_unet_features: 8-channel bf16 input rows for B tiles of N cells from the
  *   elevation, steepest slope, drainage counts, per-tile rainfall and Manning n;
  *   stats receives each tile's elevation mean and 1/std (2 floats per tile).
- * pff_unet_h0: h0 = max(exp(pred) - eps, 0); pff_unet_target: log(max(h,0) + eps). */
+ * pff_unet_h0: h0 = max(exp(pred) - eps, 0), and the water surface zh = z + h0 if zh is
+ *   not NULL; pff_unet_target: log(max(h,0) + eps). */
 int pff_conv3x3_fwd(const uint16_t *x, int csx, int offx, const uint16_t *w, const float *bias, void *y,
                     int csy, int offy, int B, int H, int W, int Cin, int Cout, int relu, int out_f32,
                     void *stream);
@@ -262,7 +269,8 @@ int pff_f32_to_bf16(const float *src, uint16_t *dst, long long n, void *stream);
 int pff_unet_features(const float *z, const float *slope, const uint32_t *counts, const float *prec,
                       const float *manning, float dx, int B, long long N, float *stats, uint16_t *out,
                       void *stream);
-int pff_unet_h0(const float *pred, int cs, float *h0, long long P, float eps, void *stream);
+int pff_unet_h0(const float *pred, int cs, float *h0, long long P, float eps, const float *z, float *zh,
+                void *stream);
 int pff_unet_target(const float *h, float *target, long long P, float eps, void *stream);
 
 #ifdef __cplusplus

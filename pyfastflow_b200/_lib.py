@@ -39,6 +39,7 @@ SIGNATURES = {
     "pff_diffuse_workspace_bytes": (_sz, [_i32]),
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
+    "pff_abs_diff_stats": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "pff_batch_workspace_bytes": (_sz, [_i64, _i32]),
     "pff_batch_plan": (_i64, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
     "pff_batch_route": (_i32, [_vp] * 5 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),
@@ -58,7 +59,7 @@ SIGNATURES = {
     "pff_adam": (_i32, [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _f32, _i32, _f32, _vp]),
     "pff_f32_to_bf16": (_i32, [_vp, _vp, _i64, _vp]),
     "pff_unet_features": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _i32, _i64, _vp, _vp, _vp]),
-    "pff_unet_h0": (_i32, [_vp, _i32, _vp, _i64, _f32, _vp]),
+    "pff_unet_h0": (_i32, [_vp, _i32, _vp, _i64, _f32, _vp, _vp, _vp]),
     "pff_unet_target": (_i32, [_vp, _vp, _i64, _f32, _vp]),
 }
 

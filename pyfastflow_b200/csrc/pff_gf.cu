@@ -4,6 +4,7 @@
 // All f32 arithmetic is written with explicit round-to-nearest intrinsics (and
 // the library is built with -fmad=false), so each operation is the reference's
 // single IEEE operation in the reference's order.
+#include <algorithm>
 #include "pff_internal.h"
 
 namespace pff {
@@ -152,6 +153,27 @@ __global__ void __launch_bounds__(256) k_core2(float *h, float *zh, const float 
         unsigned b = 0;
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) b = max(b, wm[k]);
         if (b) atomicMax(reinterpret_cast<unsigned int *>(dhmax), b);
+    }
+}
+
+// out[0] = max |a - b| (as unsigned bits: NaN above every finite value), out[1] += sum |a - b|
+__global__ void __launch_bounds__(256) k_abs_diff_stats(const float *__restrict__ a, const float *__restrict__ b, int N,
+                                                        float *out)
+{
+    unsigned mu = 0;
+    float s = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float d = fabsf(__fsub_rn(a[i], b[i]));
+        mu = max(mu, __float_as_uint(d));
+        s += d;
+    }
+    for (int o = 16; o; o >>= 1) {
+        mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (mu) atomicMax(reinterpret_cast<unsigned int *>(out), mu);
+        atomicAdd(out + 1, s);
     }
 }
 
@@ -320,4 +342,13 @@ extern "C" int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t
     { k_core1<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, rec, Q, N, dx, dx2, manning, edgesw, dt); count_launch(); }
     { k_core2<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, h_ref, dhmax, N); count_launch(); }
     return check_cuda("pff_graphflood_core");
+}
+
+extern "C" int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *stream)
+{
+    clear_error();
+    if (!a || !b || !out || N <= 0) { set_error("pff_abs_diff_stats: bad arguments"); return PFF_ERR_ARG; }
+    const int blocks = std::min(div_up(N, 256), 148 * 8);
+    { k_abs_diff_stats<<<blocks, 256, 0, S(stream)>>>(a, b, N, out); count_launch(); }
+    return check_cuda("pff_abs_diff_stats");
 }

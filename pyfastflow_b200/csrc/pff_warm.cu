@@ -87,11 +87,16 @@ __global__ void k_unet_features(const float *__restrict__ z, const float *__rest
     }
 }
 
-// h0 = max(exp(pred) - eps, 0) from channel 0 of rows of cs floats
-__global__ void k_unet_h0(const float *__restrict__ pred, int cs, float *h0, long long P, float eps)
+// h0 = max(exp(pred) - eps, 0) from channel 0 of rows of cs floats; with a bed z, also
+// the water surface zh = z + h0 (GraphFlood's state holds the surface, not the bed)
+__global__ void k_unet_h0(const float *__restrict__ pred, int cs, float *h0, long long P, float eps,
+                          const float *__restrict__ z, float *zh)
 {
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
-        h0[p] = fmaxf(expf(pred[p * cs]) - eps, 0.f);
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+        const float h = fmaxf(expf(pred[p * cs]) - eps, 0.f);
+        h0[p] = h;
+        if (zh) zh[p] = __fadd_rn(z[p], h);
+    }
 }
 
 // target = log(max(h, 0) + eps); a NaN depth counts as dry
@@ -124,15 +129,16 @@ extern "C" int pff_unet_features(const float *z, const float *slope, const uint3
     return check_cuda("pff_unet_features");
 }
 
-extern "C" int pff_unet_h0(const float *pred, int cs, float *h0, long long P, float eps, void *stream)
+extern "C" int pff_unet_h0(const float *pred, int cs, float *h0, long long P, float eps, const float *z, float *zh,
+                           void *stream)
 {
     clear_error();
-    if (!pred || !h0 || P <= 0 || cs <= 0) {
+    if (!pred || !h0 || P <= 0 || cs <= 0 || (zh && !z)) {
         set_error("pff_unet_h0: bad arguments");
         return PFF_ERR_ARG;
     }
     const int blocks = (int)std::min<long long>((P + 255) / 256, 148LL * 16);
-    { k_unet_h0<<<blocks, 256, 0, S(stream)>>>(pred, cs, h0, P, eps); count_launch(); }
+    { k_unet_h0<<<blocks, 256, 0, S(stream)>>>(pred, cs, h0, P, eps, z, zh); count_launch(); }
     return check_cuda("pff_unet_h0");
 }
 

@@ -100,9 +100,12 @@ def train(net: UNet, x, tgt, side, epochs=20, batch=16, lr=2e-3, seed=0, log=Non
     return hist
 
 
-def predict_h0(net: UNet, x, B, H, W):
-    """Initial depth (f32, B*H*W) predicted from the input rows x."""
+def predict_h0(net: UNet, x, B, H, W, z=None, zh=None):
+    """Initial depth (f32, B*H*W) predicted from the input rows x.  With the bed z
+    and an output zh (f32, B*H*W), also writes the water surface zh = z + h0, the
+    GraphFlood state that goes with that depth."""
     pred = net.forward(x, B, H, W)
     h0 = torch.empty(B * H * W, dtype=torch.float32, device=x.device)
-    _lib.call("pff_unet_h0", pred.data_ptr(), 8, h0.data_ptr(), B * H * W, EPS, _dev.stream())
+    _lib.call("pff_unet_h0", pred.data_ptr(), 8, h0.data_ptr(), B * H * W, EPS,
+              z.data_ptr() if zh is not None else None, zh.data_ptr() if zh is not None else None, _dev.stream())
     return h0

@@ -247,6 +247,13 @@ int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts
 int pff_conv3x3_fwd(const uint16_t *x, int csx, int offx, const uint16_t *w, const float *bias, void *y,
                     int csy, int offy, int B, int H, int W, int Cin, int Cout, int relu, int out_f32,
                     void *stream);
+/* Which kernel pff_conv3x3_fwd uses: 0 automatic (tcgen05 when Cin, Cout, the input
+ * offset are multiples of 64 and a 128-pixel block tiles the image, else mma.sync),
+ * 1 mma.sync only (the default), 2 tcgen05 only (PFF_ERR_ARG if unsupported).
+ * pff_conv_tc_status: 1 if a tcgen05 launch since the last call gave up waiting on
+ * its pipeline (results then unspecified), else 0; synchronizes the device. */
+int pff_conv_set_path(int path);
+int pff_conv_tc_status(int *flag);
 int pff_conv3x3_wflip(const uint16_t *w, uint16_t *wt, int Cin, int Cout, void *stream);
 int pff_conv3x3_wgrad(const uint16_t *x, int csx, int offx, const uint16_t *dy, int csd, int offd, float *dw,
                       int B, int H, int W, int Cin, int Cout, void *stream);

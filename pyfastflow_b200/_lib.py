@@ -47,6 +47,8 @@ SIGNATURES = {
     "pff_batch_graphflood": (_i32, [_vp, _vp, _vp, _vp, _f32, _f32, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32,
                                     _i32, _vp, _sz, _vp]),
     "pff_conv3x3_fwd": (_i32, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32] + [_i32] * 7 + [_vp]),
+    "pff_conv_set_path": (_i32, [_i32]),
+    "pff_conv_tc_status": (_i32, [C.POINTER(C.c_int)]),
     "pff_conv3x3_wflip": (_i32, [_vp, _vp, _i32, _i32, _vp]),
     "pff_conv3x3_wgrad": (_i32, [_vp, _i32, _i32, _vp, _i32, _i32, _vp] + [_i32] * 5 + [_vp]),
     "pff_bias_grad": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp]),

@@ -514,6 +514,13 @@ static int grid_for(long long n, int threads = 256)
     return (int)std::max<long long>(1, std::min<long long>(b, 148LL * 16));
 }
 
+// the tcgen05 forward (pff_conv_tc.cu)
+int conv_path();
+bool conv_tc_supported(int H, int W, int Cin, int Cout, int csx, int offx, int csy, int offy, int out_f32, int *BW,
+                       int *BH);
+int conv3x3_tc(const bf16_t *x, int csx, int offx, const bf16_t *w, const float *bias, void *y, int csy, int offy,
+               int B, int H, int W, int Cin, int Cout, int relu, int out_f32, cudaStream_t st);
+
 static int check_slice(const char *who, int cs, int off, int C)
 {
     if (cs <= 0 || off < 0 || C <= 0 || off + C > cs) {
@@ -542,6 +549,11 @@ extern "C" int pff_conv3x3_fwd(const bf16_t *x, int csx, int offx, const bf16_t 
         set_error("pff_conv3x3_fwd: bf16 output needs even Cout, row stride and offset");
         return PFF_ERR_ARG;
     }
+    const int path = conv_path();
+    int bw, bh;
+    const bool tc_ok = conv_tc_supported(H, W, Cin, Cout, csx, offx, csy, offy, out_f32, &bw, &bh);
+    if (path == 2 || (path == 0 && tc_ok))
+        return conv3x3_tc(x, csx, offx, w, bias, y, csy, offy, B, H, W, Cin, Cout, relu, out_f32, S(stream));
     ConvArgs a{x, csx, offx, w, bias, y, csy, offy, B, H, W, Cin, Cout, relu, out_f32};
     const long long P = (long long)B * H * W;
     dim3 grid((unsigned)((P + CV_BM - 1) / CV_BM), (unsigned)((Cout + CV_BN - 1) / CV_BN));

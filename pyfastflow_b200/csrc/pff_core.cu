@@ -78,6 +78,7 @@ __device__ __forceinline__ void rcv_pick(float zi, const float (&zn)[4], const i
 }
 
 constexpr int RCV_ROWS = 32;
+constexpr int RCV_AHEAD = 4;  // rows loaded per group (RCV_ROWS is a multiple)
 
 template <int MODE>
 __global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, int32_t *__restrict__ rcv,
@@ -93,42 +94,58 @@ __global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, 
     const int row1 = min(row0 + RCV_ROWS, g.ny);
     const bool incol = col < g.nx;
     const int nx = g.nx;
-    // register window: above, centre, below (column `col`)
-    float za = 0.f, zc = 0.f, zb = 0.f;
+    // register window: above, centre, below (column `col`); rows are loaded in groups
+    // of RCV_AHEAD so that several loads per warp are in flight
+    float za = 0.f, zc = 0.f;
     if (incol) {
         zc = __ldg(z + (size_t)row0 * nx + col);
         if (row0 > 0) za = __ldg(z + (size_t)(row0 - 1) * nx + col);
     }
-    for (int row = row0; row < row1; ++row) {
-        const int i = row * nx + col;
-        if (incol && row + 1 < g.ny) zb = __ldg(z + (size_t)(row + 1) * nx + col);
-        // left/right from the neighbouring lanes; strip-edge lanes load their own
-        float zl = __shfl_up_sync(0xffffffffu, zc, 1);
-        float zr = __shfl_down_sync(0xffffffffu, zc, 1);
-        if (incol) {
-            if (lane == 0 && col > 0) zl = __ldg(z + i - 1);
-            if ((lane == 31 || col == nx - 1) && col + 1 < nx) zr = __ldg(z + i + 1);
-            int r = i;
-            float sr = 0.f;
-            if (MODE != 3 && row > 0 && row < g.ny - 1 && col > 0 && col < nx - 1) {
-                const float zn[4] = {za, zl, zr, zb};
-                const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
-                rcv_pick(zc, zn, jn, dx, r, sr);
-            } else {
-                int jn[4];
-                float zn[4];
+    const bool hl = lane == 0 && col > 0 && incol;                                 // loads its left halo
+    const bool hr = (lane == 31 || col == nx - 1) && col + 1 < nx && incol;        // loads its right halo
+    for (int row = row0; row < row1; row += RCV_AHEAD) {
+        float zq[RCV_AHEAD], ql[RCV_AHEAD], qr[RCV_AHEAD];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    jn[k] = neighbour<MODE>(g, i, row, col, k);
-                    zn[k] = jn[k] != -1 ? __ldg(z + jn[k]) : 0.f;
-                }
-                rcv_pick(zc, zn, jn, dx, r, sr);
-            }
-            rcv[i] = r;
-            grad[i] = sr;
+        for (int q = 0; q < RCV_AHEAD; ++q) {
+            const int rb = row + 1 + q, rc = row + q;
+            zq[q] = (incol && rb < g.ny && rb <= row1) ? __ldg(z + (size_t)rb * nx + col) : 0.f;
+            ql[q] = (hl && rc < row1) ? __ldg(z + (size_t)rc * nx + col - 1) : 0.f;
+            qr[q] = (hr && rc < row1) ? __ldg(z + (size_t)rc * nx + col + 1) : 0.f;
         }
-        za = zc;
-        zc = zb;
+#pragma unroll
+        for (int q = 0; q < RCV_AHEAD; ++q) {
+            const int rw = row + q;
+            if (rw >= row1) break;
+            const int i = rw * nx + col;
+            const float zb = zq[q];
+            // left/right from the neighbouring lanes; strip-edge lanes use their halo loads
+            float zl = __shfl_up_sync(0xffffffffu, zc, 1);
+            float zr = __shfl_down_sync(0xffffffffu, zc, 1);
+            if (hl) zl = ql[q];
+            if (hr) zr = qr[q];
+            if (incol) {
+                int r = i;
+                float sr = 0.f;
+                if (MODE != 3 && rw > 0 && rw < g.ny - 1 && col > 0 && col < nx - 1) {
+                    const float zn[4] = {za, zl, zr, zb};
+                    const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                    rcv_pick(zc, zn, jn, dx, r, sr);
+                } else {
+                    int jn[4];
+                    float zn[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        jn[k] = neighbour<MODE>(g, i, rw, col, k);
+                        zn[k] = jn[k] != -1 ? __ldg(z + jn[k]) : 0.f;
+                    }
+                    rcv_pick(zc, zn, jn, dx, r, sr);
+                }
+                rcv[i] = r;
+                grad[i] = sr;
+            }
+            za = zc;
+            zc = zb;
+        }
     }
 }
 

@@ -500,6 +500,7 @@ __global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restri
 // left/right values from neighbouring lanes.  Border cells of pit basins collect
 // in a per-warp shared buffer, flushed with one atomic per strip.
 constexpr int SAD_ROWS = 32;
+constexpr int SAD_AHEAD = 4;  // rows loaded per group (SAD_ROWS is a multiple)
 
 template <int MODE>
 __device__ __forceinline__ bool saddle_cell(int i, int row, int col, const Grid &g, int bi, float zi, const int (&jn)[4],
@@ -544,48 +545,70 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
     const int row1 = min(row0 + SAD_ROWS, ny);
     const bool incol = col < nx;
     int nb = 0;  // border cells buffered by this warp
-    int ba = 0, bc = 0, bb = 0;
-    float za = 0.f, zc = 0.f, zb = 0.f;
+    int ba = 0, bc = 0;
+    float za = 0.f, zc = 0.f;
     if (incol) {
         bc = bid[row0 * nx + col];
         zc = z[row0 * nx + col];
         if (row0 > 0) { ba = bid[(row0 - 1) * nx + col]; za = z[(row0 - 1) * nx + col]; }
     }
-    for (int row = row0; row < row1; ++row) {
-        const int i = row * nx + col;
-        if (incol && row + 1 < ny) { bb = bid[i + nx]; zb = z[i + nx]; }
-        int bl = __shfl_up_sync(0xffffffffu, bc, 1), br = __shfl_down_sync(0xffffffffu, bc, 1);
-        float zl = __shfl_up_sync(0xffffffffu, zc, 1), zr = __shfl_down_sync(0xffffffffu, zc, 1);
-        bool listed = false;
-        if (incol) {
-            const bool interior = MODE != 3 && row > 0 && row < ny - 1 && col > 0 && col < nx - 1;
-            if (interior) {
-                if (lane == 0) { bl = bid[i - 1]; zl = z[i - 1]; }
-                if (lane == 31) { br = bid[i + 1]; zr = z[i + 1]; }
-                // interior cells of modes 0-2 never leave the domain
-                const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
-                const int bn[4] = {ba, bl, br, bb};
-                const float zn[4] = {za, zl, zr, zb};
-                listed = saddle_cell<MODE>(i, row, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
-            } else if (can_leave<MODE>(g, i, row, col)) {
-                zp[i] = zc;
-            } else {
-                int jn[4], bn[4];
-                float zn[4];
-                neighbours4<MODE>(g, i, row, col, jn);
+    const bool hl = lane == 0 && col > 0 && incol, hr = lane == 31 && col + 1 < nx && incol;
+    for (int row = row0; row < row1; row += SAD_AHEAD) {
+        // the rows below (and the strip-edge halo) of SAD_AHEAD rows, loaded together
+        int bq[SAD_AHEAD], lq[SAD_AHEAD], rq[SAD_AHEAD];
+        float zq[SAD_AHEAD], zlq[SAD_AHEAD], zrq[SAD_AHEAD];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    bn[k] = jn[k] != -1 ? bid[jn[k]] : 0;
-                    zn[k] = jn[k] != -1 ? z[jn[k]] : 0.f;
-                }
-                listed = saddle_cell<MODE>(i, row, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
-            }
+        for (int q = 0; q < SAD_AHEAD; ++q) {
+            const int rb = row + 1 + q, rc = row + q;
+            const bool vb = incol && rb < ny && rb <= row1;
+            bq[q] = vb ? bid[rb * nx + col] : 0;
+            zq[q] = vb ? z[rb * nx + col] : 0.f;
+            const bool vl = hl && rc < row1, vr = hr && rc < row1;
+            lq[q] = vl ? bid[rc * nx + col - 1] : 0;
+            zlq[q] = vl ? z[rc * nx + col - 1] : 0.f;
+            rq[q] = vr ? bid[rc * nx + col + 1] : 0;
+            zrq[q] = vr ? z[rc * nx + col + 1] : 0.f;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, listed);
-        if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = i;
-        nb += __popc(m);
-        ba = bc; bc = bb;
-        za = zc; zc = zb;
+#pragma unroll
+        for (int q = 0; q < SAD_AHEAD; ++q) {
+            const int rw = row + q;
+            if (rw >= row1) break;
+            const int i = rw * nx + col;
+            const int bb = bq[q];
+            const float zb = zq[q];
+            int bl = __shfl_up_sync(0xffffffffu, bc, 1), br = __shfl_down_sync(0xffffffffu, bc, 1);
+            float zl = __shfl_up_sync(0xffffffffu, zc, 1), zr = __shfl_down_sync(0xffffffffu, zc, 1);
+            bool listed = false;
+            if (incol) {
+                const bool interior = MODE != 3 && rw > 0 && rw < ny - 1 && col > 0 && col < nx - 1;
+                if (interior) {
+                    if (lane == 0) { bl = lq[q]; zl = zlq[q]; }
+                    if (lane == 31) { br = rq[q]; zr = zrq[q]; }
+                    // interior cells of modes 0-2 never leave the domain
+                    const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                    const int bn[4] = {ba, bl, br, bb};
+                    const float zn[4] = {za, zl, zr, zb};
+                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+                } else if (can_leave<MODE>(g, i, rw, col)) {
+                    zp[i] = zc;
+                } else {
+                    int jn[4], bn[4];
+                    float zn[4];
+                    neighbours4<MODE>(g, i, rw, col, jn);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        bn[k] = jn[k] != -1 ? bid[jn[k]] : 0;
+                        zn[k] = jn[k] != -1 ? z[jn[k]] : 0.f;
+                    }
+                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, listed);
+            if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = i;
+            nb += __popc(m);
+            ba = bc; bc = bb;
+            za = zc; zc = zb;
+        }
     }
     __syncwarp();
     int base = 0;

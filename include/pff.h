@@ -249,7 +249,7 @@ int pff_conv3x3_fwd(const uint16_t *x, int csx, int offx, const uint16_t *w, con
                     void *stream);
 /* Which kernel pff_conv3x3_fwd uses: 0 automatic (tcgen05 when Cin, Cout, the input
  * offset are multiples of 64 and a 128-pixel block tiles the image, else mma.sync),
- * 1 mma.sync only (the default), 2 tcgen05 only (PFF_ERR_ARG if unsupported).
+ * 1 mma.sync only, 2 tcgen05 only (PFF_ERR_ARG if unsupported).  Default 0.
  * pff_conv_tc_status: 1 if a tcgen05 launch since the last call gave up waiting on
  * its pipeline (results then unspecified), else 0; synchronizes the device. */
 int pff_conv_set_path(int path);

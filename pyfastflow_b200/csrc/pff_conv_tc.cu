@@ -269,7 +269,7 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-static int g_conv_path = 1;  // 0 automatic, 1 mma.sync only (default), 2 tcgen05 only
+static int g_conv_path = 0;  // 0 automatic (default), 1 mma.sync only, 2 tcgen05 only
 static int *g_tc_err[64] = {nullptr};
 
 // Whether the tcgen05 kernel applies: channel counts, slice offsets and a pixel block

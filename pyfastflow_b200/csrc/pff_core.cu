@@ -79,6 +79,7 @@ __device__ __forceinline__ void rcv_pick(float zi, const float (&zn)[4], const i
 
 constexpr int RCV_ROWS = 32;
 constexpr int RCV_AHEAD = 4;  // rows loaded per group (RCV_ROWS is a multiple)
+constexpr int RCV4_ROWS = 8;  // rows per warp of the 4-column kernel (a multiple of RCV_AHEAD)
 
 template <int MODE>
 __global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, int32_t *__restrict__ rcv,
@@ -149,10 +150,132 @@ __global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, 
     }
 }
 
+// The same choice with one division: the reference's sequential strict '>' keeps the
+// first direction whose rounded quotient equals the largest rounded quotient, and
+// by monotonicity that largest quotient is fl(dmax / dx).  Another direction can
+// tie with it after rounding only if its drop lies within a few ulps of dmax, so
+// only such near-ties pay a second division.
+__device__ __forceinline__ void rcv_pick1(float zi, const float (&zn)[4], const int (&jn)[4], float dx, int &r,
+                                          float &sr)
+{
+    float d[4], dmax = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        d[k] = jn[k] != -1 ? __fsub_rn(zi, zn[k]) : 0.f;
+        if (d[k] > dmax) dmax = d[k];
+    }
+    if (!(dmax > 0.f)) return;
+    const float q = __fdiv_rn(dmax, dx);
+    if (!(q > 0.f)) return;
+    const float near = __fmul_rn(dmax, 1.0f - 0x1p-21f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!(d[k] >= near)) continue;  // also skips invalid directions (d = 0 < near) and NaN
+        if (d[k] == dmax || __fdiv_rn(d[k], dx) == q) {
+            r = jn[k];
+            sr = q;
+            return;
+        }
+    }
+}
+
+// Four columns per thread: a warp covers a 128-column strip, rows in groups of
+// RCV_AHEAD; float4 loads and int4 / float4 stores; left and right neighbours from
+// the adjacent lanes.  Needs nx % 4 == 0 (16-byte aligned rows).
+template <int MODE>
+__global__ void __launch_bounds__(128) k_receivers4(const float *__restrict__ z, int32_t *__restrict__ rcv,
+                                                    float *__restrict__ grad, Grid g, float dx)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nx = g.nx, ny = g.ny;
+    const int nstrips = (nx + 127) >> 7;
+    const int strip = warp % nstrips, band = warp / nstrips;
+    const int c0 = (strip << 7) + 4 * lane;  // first of this thread's 4 columns
+    const int row0 = band * RCV4_ROWS;
+    if (row0 >= ny) return;
+    const int row1 = min(row0 + RCV4_ROWS, ny);
+    const bool incol = c0 < nx;  // nx % 4 == 0: all 4 columns are in
+    const float4 *z4 = reinterpret_cast<const float4 *>(z);
+    const int nx4 = nx >> 2;
+    const int q0 = c0 >> 2;
+    float4 za = make_float4(0.f, 0.f, 0.f, 0.f), zc = za;
+    if (incol) {
+        zc = __ldg(z4 + (size_t)row0 * nx4 + q0);
+        if (row0 > 0) za = __ldg(z4 + (size_t)(row0 - 1) * nx4 + q0);
+    }
+    const bool hl = lane == 0 && c0 > 0 && incol;                         // left halo from memory
+    const bool hr = (lane == 31 || c0 + 4 >= nx) && c0 + 4 < nx && incol;  // right halo from memory
+    for (int row = row0; row < row1; row += RCV_AHEAD) {
+        float4 zq[RCV_AHEAD];
+        float ql[RCV_AHEAD], qr[RCV_AHEAD];
+#pragma unroll
+        for (int q = 0; q < RCV_AHEAD; ++q) {
+            const int rb = row + 1 + q, rc = row + q;
+            zq[q] = (incol && rb < ny && rb <= row1) ? __ldg(z4 + (size_t)rb * nx4 + q0) : make_float4(0.f, 0.f, 0.f, 0.f);
+            ql[q] = (hl && rc < row1) ? __ldg(z + (size_t)rc * nx + c0 - 1) : 0.f;
+            qr[q] = (hr && rc < row1) ? __ldg(z + (size_t)rc * nx + c0 + 4) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < RCV_AHEAD; ++q) {
+            const int rw = row + q;
+            if (rw >= row1) break;
+            const float4 zb = zq[q];
+            float zl = __shfl_up_sync(0xffffffffu, zc.w, 1);
+            float zr = __shfl_down_sync(0xffffffffu, zc.x, 1);
+            if (hl) zl = ql[q];
+            if (hr) zr = qr[q];
+            if (incol) {
+                const float cz[4] = {zc.x, zc.y, zc.z, zc.w};
+                const float az[4] = {za.x, za.y, za.z, za.w};
+                const float bz[4] = {zb.x, zb.y, zb.z, zb.w};
+                int rr[4];
+                float ss[4];
+                const bool rowin = MODE != 3 && rw > 0 && rw < ny - 1;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int col = c0 + k;
+                    const int i = rw * nx + col;
+                    int r = i;
+                    float sr = 0.f;
+                    if (rowin && col > 0 && col < nx - 1) {
+                        const float zn[4] = {az[k], k > 0 ? cz[k - 1] : zl, k < 3 ? cz[k + 1] : zr, bz[k]};
+                        const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                        rcv_pick1(cz[k], zn, jn, dx, r, sr);
+                    } else {
+                        int jn[4];
+                        float zn[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            jn[m] = neighbour<MODE>(g, i, rw, col, m);
+                            zn[m] = jn[m] != -1 ? __ldg(z + jn[m]) : 0.f;
+                        }
+                        rcv_pick1(cz[k], zn, jn, dx, r, sr);
+                    }
+                    rr[k] = r;
+                    ss[k] = sr;
+                }
+                const size_t o = (size_t)rw * nx4 + q0;
+                reinterpret_cast<int4 *>(rcv)[o] = make_int4(rr[0], rr[1], rr[2], rr[3]);
+                reinterpret_cast<float4 *>(grad)[o] = make_float4(ss[0], ss[1], ss[2], ss[3]);
+            }
+            za = zc;
+            zc = zb;
+        }
+    }
+}
+
 template <int MODE>
 static void launch_receivers(const float *z, int32_t *rcv, float *grad, const Grid &g, float dx,
                              cudaStream_t st)
 {
+    const bool vec = g.nx % 4 == 0 && ((uintptr_t)z % 16) == 0 && ((uintptr_t)rcv % 16) == 0 &&
+                     ((uintptr_t)grad % 16) == 0;
+    if (vec) {
+        const long long warps = (long long)((g.nx + 127) / 128) * ((g.ny + RCV4_ROWS - 1) / RCV4_ROWS);
+        { k_receivers4<MODE><<<div_up(warps, 4), 128, 0, st>>>(z, rcv, grad, g, dx); count_launch(); }
+        return;
+    }
     const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + RCV_ROWS - 1) / RCV_ROWS);
     { k_receivers<MODE><<<div_up(warps, 4), 128, 0, st>>>(z, rcv, grad, g, dx); count_launch(); }
 }

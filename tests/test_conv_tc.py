@@ -33,6 +33,7 @@ def test_conv_path_switch_host_checks():
     lib = _lib.load()
     assert lib.pff_conv_set_path(3) != 0
     assert lib.pff_conv_set_path(1) == 0
+    assert lib.pff_conv_set_path(0) == 0  # back to the default
 
 
 @pytest.mark.gpu
@@ -71,7 +72,7 @@ def test_tcgen05_conv_matches(cuda, B, H, W, Cin, Cout, cs_in, off_in, relu, f32
         _lib.call("pff_conv_tc_status", C.byref(flag))
         assert flag.value == 0, "a tcgen05 pipeline wait gave up"
     finally:
-        lib.pff_conv_set_path(1)
+        lib.pff_conv_set_path(0)
     tol = 2e-5 * np.sqrt(9 * Cin) + 1e-5 if f32 else 1e-2
     scale = float(ref.abs().max())
     assert float((outs[2] - ref).abs().max()) / scale < tol
@@ -92,4 +93,4 @@ def test_tcgen05_rejects_unsupported(cuda):
                                  _dev.stream())
         assert rc != 0  # Cin = 32 is not a multiple of 64
     finally:
-        lib.pff_conv_set_path(1)
+        lib.pff_conv_set_path(0)

@@ -149,6 +149,7 @@ def main():
     ap.add_argument("--tiles", type=int, default=512)
     ap.add_argument("--no-per-tile", action="store_true", help="ragged: skip the per-tile comparison arm")
     ap.add_argument("--no-tune", action="store_true", help="ragged: fixed 1024 threads x 1 CTA per SM")
+    ap.add_argument("--per-layer", action="store_true", help="conv: also time every layer on both kernels")
     ap.add_argument("--max-iter", type=int, default=20000)
     ap.add_argument("--fp64-size", type=int, default=256)
     ap.add_argument("--fp64-iters", type=int, default=200)
@@ -272,18 +273,19 @@ def main():
     wh = torch.from_numpy(w).pin_memory()
     qh = torch.empty(n * n, dtype=torch.float32).pin_memory()
     ch = torch.empty(n * n, dtype=torch.int32).pin_memory()
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(2, min(args.steps, 8))
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # one DEM per step through FlowRouter.route_many: every step copies its DEM and
+    # weights in and its Q and counts out; the copies of neighbouring steps overlap
+    # the routing on two copy streams
+    qhs = [qh] * e2e_steps
+    chs = [ch] * e2e_steps
+    router.route_many([zh] * 2, [wh] * 2, qhs[:2], chs[:2])  # untimed: creates the copy streams and buffers
+    torch.cuda.synchronize()
+    barrier()
     e0.record()
-    for s in range(e2e_steps):
-        router.z.copy_(zh, non_blocking=True)
-        router.Q.copy_(wh, non_blocking=True)
-        router.compute_receivers()
-        router.reroute_flow()
-        router._accumulate(True)
-        qh.copy_(router.Q, non_blocking=True)
-        ch.copy_(router.counts, non_blocking=True)
+    router.route_many([zh] * e2e_steps, [wh] * e2e_steps, qhs, chs)
     e1.record()
     barrier()
     e2e_ms = e0.elapsed_time(e1)
@@ -299,7 +301,8 @@ def main():
                           n_outer_reroute=router.last_n_outer),
            "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(launches),
            "e2e": {"value": e2e_v, "unit": "Mcells/s", "h2d_bytes_per_step": 8 * n * n,
-                   "d2h_bytes_per_step": 8 * n * n, "steps": e2e_steps}}
+                   "d2h_bytes_per_step": 8 * n * n, "steps": e2e_steps,
+                   "api": "FlowRouter.route_many (copies of neighbouring steps overlap the routing)"}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sn, zs, ws, used = cpu_sample(threads)
@@ -481,7 +484,10 @@ def conv_main(args):
         peak, src = float(pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))), "measured"
     except Exception:
         peak, src = 1400.0, "fallback"
-    print(json.dumps({"metric": CONV_METRIC, "value": tf, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+    layers = None
+    if args.per_layer:
+        layers = conv_per_layer(B, H, W)
+    print(json.dumps({"metric": CONV_METRIC, "value": tf, "per_layer": layers, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
                       "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": "bf16",
                       "data": "synthetic", "config": {"workload": f"U-Net step, batch {B} x {H} x {W}",
                                                       "conv_gflop_per_step": flops / 1e9},
@@ -620,6 +626,56 @@ def warmstart_main(args):
                         "loss_last": hist[-1]},
            "log": logs}
     print(json.dumps(out))
+
+
+def conv_per_layer(B, H, W, reps=10):
+    """Forward time of every U-Net layer shape on the mma.sync kernel and (where it
+    applies) the tcgen05 kernel, and the weight gradient, L2 flushed between runs."""
+    import torch
+
+    from pyfastflow_b200 import _dev, _lib
+    from pyfastflow_b200.warmstart import LAYERS
+
+    lib = _lib.load()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timeit(fn):
+        for _ in range(3):
+            fn()
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts)) * 1e3
+
+    out = {}
+    for name, _, _, _, _, cin, cout, _, lev in LAYERS:
+        h, w = H >> lev, W >> lev
+        P = B * h * w
+        x = (torch.randn(P * cin) * 0.5).to(torch.bfloat16).cuda()
+        wt = (torch.randn(cout * 9 * cin) * 0.05).to(torch.bfloat16).cuda()
+        y = torch.empty(P * cout, dtype=torch.bfloat16, device="cuda")
+        fl = 2.0 * cin * cout * 9 * P
+        row = {"shape": f"{B}x{h}x{w} {cin}->{cout}"}
+        for path, key in ((1, "mma_sync_us"), (2, "tcgen05_us")):
+            lib.pff_conv_set_path(path)
+            try:
+                row[key] = timeit(lambda: _lib.call("pff_conv3x3_fwd", x.data_ptr(), cin, 0, wt.data_ptr(), None,
+                                                    y.data_ptr(), cout, 0, B, h, w, cin, cout, 1, 0, _dev.stream()))
+                row[key.replace("_us", "_tflops")] = fl / row[key] / 1e6
+            except _lib.PFFError:
+                row[key] = None
+        lib.pff_conv_set_path(0)
+        dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device="cuda")
+        row["wgrad_us"] = timeit(lambda: _lib.call("pff_conv3x3_wgrad", x.data_ptr(), cin, 0, y.data_ptr(), cout, 0,
+                                                   dw.data_ptr(), B, h, w, cin, cout, _dev.stream()))
+        out[name] = row
+    return out
 
 
 GF_METRIC = "graphflood s-to-residual"

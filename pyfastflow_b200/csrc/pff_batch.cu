@@ -312,8 +312,16 @@ __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_
 }
 
 // ---- reroute_carve (lakeflow.py:308-438); leaves the result in rec and rec_ ----------
-__device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *rec__, int32_t *claim, uint8_t *tag,
-                           uint8_t *tag_, const int32_t *snode, const long long *out, int *status)
+//
+// The reference tags the saddle nodes and propagates the tags by pointer jumping until
+// no tag changes; a round adds the next 2^r cells of every tagged path, so the fixed
+// point is the union of the saddle nodes' forward orbits under rec_ (down to each
+// pit, or around a receiver cycle).  The jumped pointers are discarded by the
+// finalisation, so only that tag set matters: here each saddle node walks its own
+// orbit, stopping at a cell already tagged (the rest of that orbit is another
+// walker's) or at a root.
+__device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *claim, uint8_t *tag, const int32_t *snode,
+                           const long long *out, int *status)
 {
     const long long iv = inv_key();
     FOR_CELLS(i, N) {
@@ -321,42 +329,24 @@ __device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *rec__, i
         claim[i] = -1;
     }
     __syncthreads();
+    int overrun = 0;
     FOR_CELLS(b, N) {
-        const int s = snode[b];
-        if (s != -1) tag[s] = 1;
-    }
-    __syncthreads();
-    FOR_CELLS(i, N) {
-        tag_[i] = tag[i];
-        const int r = rec_[i];
-        rec[i] = r;
-        rec__[i] = r;
-    }
-    __syncthreads();
-    // until no tag changes; each productive round adds a tag, so N + 1 rounds bound it
-    int r = 0;
-    for (; r <= N + 1; ++r) {
-        FOR_CELLS(i, N) {
-            const int ri = rec[i];
-            if (tag[i]) tag_[ri] = 1;
-            rec_[i] = ri;
+        int x = snode[b];
+        if (x == -1) continue;
+        int s = 0;
+        for (; s <= N; ++s) {
+            if (tag[x]) break;
+            tag[x] = 1;
+            const int nx_ = rec_[x];
+            if (nx_ == x) break;
+            x = nx_;
         }
-        __syncthreads();
-        int ch = 0;
-        FOR_CELLS(i, N) {
-            rec[i] = rec_[rec_[i]];
-            const uint8_t t = tag_[i];
-            if (tag[i] != t) {
-                ch = 1;
-                tag[i] = t;
-            }
-        }
-        if (!__syncthreads_or(ch)) break;
+        if (s > N) overrun = 1;
     }
-    if (r > N + 1 && threadIdx.x == 0) atomicOr(status, BST_CARVE);
+    if (__syncthreads_or(overrun) && threadIdx.x == 0) atomicOr(status, BST_CARVE);
     // finalise: pre-carve receivers, path reversal (largest index wins), saddle links
     FOR_CELLS(i, N) {
-        const int r0 = rec__[i];
+        const int r0 = rec_[i];
         rec[i] = r0;
         if (tag[r0] && tag[i] && i != r0) atomicMax(claim + r0, i);
     }
@@ -384,8 +374,11 @@ __device__ __forceinline__ bool bget_src(const int32_t *src, int t, int it)
     return flip;
 }
 
+// Only nodes that still have donors are visited: a node with none left does nothing
+// in any later round, so the rounds run over a compacted active list (la -> lb).
 __device__ void tile_accumulate(int N, const int32_t *rcv, float *p, uint32_t *c, int32_t *dnr, int32_t *dnr_,
-                                int32_t *ndnr, int32_t *ndnr_, int32_t *src, float *p_, uint32_t *c_)
+                                int32_t *ndnr, int32_t *ndnr_, int32_t *src, float *p_, uint32_t *c_, int32_t *la,
+                                int32_t *lb, BatchShm &sh)
 {
     FOR_CELLS(t, N) {
         ndnr[t] = 0;
@@ -400,74 +393,98 @@ __device__ void tile_accumulate(int N, const int32_t *rcv, float *p, uint32_t *c
         if (slot < 4) dnr[4LL * r + slot] = t;
     }
     __syncthreads();
-    FOR_CELLS(r, N) {  // ascending donor index: the reference's serial slot order
-        const int n = min(ndnr[r], 4);
-        int *d = dnr + 4LL * r;
-        for (int a = 1; a < n; ++a) {
-            const int x = d[a];
-            int b = a - 1;
-            while (b >= 0 && d[b] > x) {
-                d[b + 1] = d[b];
-                --b;
+    int nact = 0;
+    for (int b0 = 0; b0 < N; b0 += blockDim.x) {  // sort donors (ascending: the serial slot order), list actives
+        const int r = b0 + threadIdx.x;
+        int f = 0;
+        if (r < N) {
+            const int n = min(ndnr[r], 4);
+            int *d = dnr + 4LL * r;
+            for (int a = 1; a < n; ++a) {
+                const int x = d[a];
+                int b = a - 1;
+                while (b >= 0 && d[b] > x) {
+                    d[b + 1] = d[b];
+                    --b;
+                }
+                d[b + 1] = x;
             }
-            d[b + 1] = x;
+            f = n > 0;
         }
+        int tot;
+        const int q = bscan(f, sh, &tot);
+        if (f) la[nact + q] = r;
+        nact += tot;
     }
     __syncthreads();
     const int logn = bceil_log2(N) + 1;
-    for (int it = 0; it <= logn; ++it) {
-        int worked_any = 0;
-        FOR_CELLS(tid, N) {
-            const bool flip = bget_src(src, tid, it);
-            int todo = flip ? ndnr_[tid] : ndnr[tid];
-            if (todo <= 0) continue;
-            const long long base = 4LL * tid;
-            int donors[4] = {-1, -1, -1, -1};
-            bool worked = false;
-            float padd = 0.f;
-            uint32_t cadd = 0;
-            int i = 0;
-            while (i < todo && i < 4) {
-                if (donors[i] == -1) donors[i] = flip ? dnr_[base + i] : dnr[base + i];
-                const int did = donors[i];
-                const bool fd = bget_src(src, did, it);
-                const int nd = fd ? ndnr_[did] : ndnr[did];
-                if (nd <= 1) {
-                    if (!worked) {
-                        padd = flip ? p_[tid] : p[tid];
-                        cadd = flip ? c_[tid] : c[tid];
+    for (int it = 0; it <= logn && nact > 0; ++it) {
+        int worked_any = 0, nnext = 0;
+        for (int b0 = 0; b0 < nact; b0 += blockDim.x) {
+            const int k = b0 + threadIdx.x;
+            int keep = 0, tid = -1;
+            if (k < nact) {
+                tid = la[k];
+                const bool flip = bget_src(src, tid, it);
+                int todo = flip ? ndnr_[tid] : ndnr[tid];
+                const long long base = 4LL * tid;
+                int donors[4] = {-1, -1, -1, -1};
+                bool worked = false;
+                float padd = 0.f;
+                uint32_t cadd = 0;
+                int i = 0;
+                while (i < todo && i < 4) {
+                    if (donors[i] == -1) donors[i] = flip ? dnr_[base + i] : dnr[base + i];
+                    const int did = donors[i];
+                    const bool fd = bget_src(src, did, it);
+                    const int nd = fd ? ndnr_[did] : ndnr[did];
+                    if (nd <= 1) {
+                        if (!worked) {
+                            padd = flip ? p_[tid] : p[tid];
+                            cadd = flip ? c_[tid] : c[tid];
+                        }
+                        worked = true;
+                        padd = __fadd_rn(padd, fd ? p_[did] : p[did]);
+                        cadd += fd ? c_[did] : c[did];
+                        if (nd == 0) {
+                            --todo;
+                            if (todo > i) donors[i] = flip ? dnr_[base + todo] : dnr[base + todo];
+                            --i;
+                        } else {
+                            donors[i] = fd ? dnr_[4LL * did] : dnr[4LL * did];
+                        }
                     }
-                    worked = true;
-                    padd = __fadd_rn(padd, fd ? p_[did] : p[did]);
-                    cadd += fd ? c_[did] : c[did];
-                    if (nd == 0) {
-                        --todo;
-                        if (todo > i) donors[i] = flip ? dnr_[base + todo] : dnr[base + todo];
-                        --i;
-                    } else {
-                        donors[i] = fd ? dnr_[4LL * did] : dnr[4LL * did];
-                    }
+                    ++i;
                 }
-                ++i;
+                if (worked) {
+                    worked_any = 1;
+                    const int m = todo < 4 ? todo : 4;
+                    if (flip) {
+                        ndnr[tid] = todo;
+                        p[tid] = padd;
+                        c[tid] = cadd;
+                        for (int j = 0; j < m; ++j) dnr[base + j] = donors[j];
+                    } else {
+                        ndnr_[tid] = todo;
+                        p_[tid] = padd;
+                        c_[tid] = cadd;
+                        for (int j = 0; j < m; ++j) dnr_[base + j] = donors[j];
+                    }
+                    src[tid] = (flip ? 1 : -1) * (it + 1);
+                }
+                keep = todo > 0;
             }
-            if (!worked) continue;
-            worked_any = 1;
-            const int m = todo < 4 ? todo : 4;
-            if (flip) {
-                ndnr[tid] = todo;
-                p[tid] = padd;
-                c[tid] = cadd;
-                for (int j = 0; j < m; ++j) dnr[base + j] = donors[j];
-            } else {
-                ndnr_[tid] = todo;
-                p_[tid] = padd;
-                c_[tid] = cadd;
-                for (int j = 0; j < m; ++j) dnr_[base + j] = donors[j];
-            }
-            src[tid] = (flip ? 1 : -1) * (it + 1);
+            int tot;
+            const int q = bscan(keep, sh, &tot);
+            if (keep) lb[nnext + q] = tid;
+            nnext += tot;
         }
         // a round in which nothing worked leaves the state, and every later round, unchanged
         if (!__syncthreads_or(worked_any)) break;
+        int32_t *t = la;
+        la = lb;
+        lb = t;
+        nact = nnext;
     }
     FOR_CELLS(t, N) {  // fuse(Q, src, Q_, logn)
         if (bget_src(src, t, logn)) {
@@ -532,7 +549,7 @@ __device__ void tile_reroute(const Grid &g, const BatchTile &T, const BatchArray
         tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
         tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
                               A.inv + ob, z);
-        tile_carve(N, rec, rec_, rec__, A.mark + o, A.tag + o, A.tag_ + o, A.snode + ob, A.outlet + ob, A.status);
+        tile_carve(N, rec, rec_, A.mark + o, A.tag + o, A.snode + ob, A.outlet + ob, A.status);
     }
 }
 
@@ -547,7 +564,7 @@ __device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &s
     tile_reroute<MODE>(g, T, A, z, sh);
     // accumulate: Q holds the seed (flowfields.py:272-292)
     tile_accumulate(N, A.rcv + o, A.Q + o, A.counts + o, A.dnr + 4 * o, A.dnr_ + 4 * o, A.ndnr + o, A.ndnr_ + o,
-                    A.src + o, A.p_ + o, A.c_ + o);
+                    A.src + o, A.p_ + o, A.c_ + o, A.mark + o, A.rec__ + o, sh);
 }
 
 // ---- GraphFlood on a tile (gf_fields.py:126-141) --------------------------------------

@@ -149,6 +149,84 @@ class FlowRouter:
         self.Q.fill_(value * (self.dx * self.dx if area else 1.0))
         self._accumulate(counts)
 
+    def route_many(self, dems, weights=None, out_Q=None, out_counts=None, carve=True):
+        """Route a sequence of DEMs of this grid: for each k, z = dems[k] ->
+        compute_receivers -> reroute_flow(carve) -> accumulate (weights[k] per cell,
+        or 1 per cell with area False) -> out_Q[k], out_counts[k].
+
+        dems, weights, out_Q, out_counts are host tensors (pinned for overlap) of N
+        elements each (counts as int32 bits of the uint32 values).  The host-to-device
+        copy of DEM k+1 and the device-to-host copy of the results of DEM k-1 run on
+        two copy streams while DEM k is routed, so a long sequence costs about the
+        routing time when the copies are shorter.  No reference counterpart (the
+        reference routes one DEM per call).  Returns when every copy has landed."""
+        n = len(dems)
+        if n == 0:
+            return
+        dev = self.device
+        main = torch.cuda.current_stream(dev)
+        if getattr(self, "_rm", None) is None:  # double buffers and copy streams, kept for later calls
+            N = self.N
+            self._rm = dict(h2d=torch.cuda.Stream(dev), d2h=torch.cuda.Stream(dev),
+                            zb=[torch.empty(N, dtype=torch.float32, device=dev) for _ in range(2)],
+                            wb=[torch.empty(N, dtype=torch.float32, device=dev) for _ in range(2)],
+                            qb=[torch.empty(N, dtype=torch.float32, device=dev) for _ in range(2)],
+                            cb=[torch.empty(N, dtype=torch.int32, device=dev) for _ in range(2)])
+        rm = self._rm
+        h2d, d2h = rm["h2d"], rm["d2h"]
+        zb, qb, cb = rm["zb"], rm["qb"], rm["cb"]
+        wb = rm["wb"] if weights is not None else None
+        h2d.wait_stream(main)  # the buffers' previous users (an earlier call) are done
+        d2h.wait_stream(main)
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_used = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [torch.cuda.Event() for _ in range(2)]
+        ev_drained = [torch.cuda.Event() for _ in range(2)]
+        start = torch.cuda.Event()
+        start.record(main)
+
+        def load(k):
+            b = k & 1
+            h2d.wait_event(start)
+            if k >= 2:
+                h2d.wait_event(ev_used[b])  # DEM k-2 has left this buffer
+            with torch.cuda.stream(h2d):
+                zb[b].copy_(dems[k].reshape(-1), non_blocking=True)
+                if wb is not None:
+                    wb[b].copy_(weights[k].reshape(-1), non_blocking=True)
+            ev_in[b].record(h2d)
+
+        load(0)
+        for k in range(n):
+            b = k & 1
+            if k + 1 < n:
+                load(k + 1)
+            main.wait_event(ev_in[b])
+            self.z.copy_(zb[b])
+            if wb is not None:
+                self.Q.copy_(wb[b])
+            else:
+                self.Q.fill_(1.0)
+            ev_used[b].record(main)
+            self.compute_receivers()
+            if self.lakeflow:
+                self.reroute_flow(carve)
+            self._accumulate(True)
+            if k >= 2:
+                main.wait_event(ev_drained[b])  # results of DEM k-2 have left this buffer
+            qb[b].copy_(self.Q)
+            cb[b].copy_(self.counts)
+            ev_out[b].record(main)
+            d2h.wait_event(ev_out[b])
+            with torch.cuda.stream(d2h):
+                if out_Q is not None:
+                    out_Q[k].reshape(-1).copy_(qb[b], non_blocking=True)
+                if out_counts is not None:
+                    out_counts[k].reshape(-1).copy_(cb[b], non_blocking=True)
+            ev_drained[b].record(d2h)
+        main.wait_stream(d2h)
+        main.wait_stream(h2d)
+
     def accumulate_weighted_Q(self, weights, counts=True):
         """Upstream sum of per-cell weights (e.g. precipitation-weighted
         discharge), the path scripts run by filling Q before rcv2donor

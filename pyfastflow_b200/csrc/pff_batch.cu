@@ -49,10 +49,14 @@ struct BatchArrays {
 
 enum : int { BST_MODE = 1, BST_CYCLE_LABELS = 8, BST_CARVE = 16 };
 
+constexpr int LB_SIDE = 32, LB_CELLS = LB_SIDE * LB_SIDE;  // label sub-blocks
+
 struct BatchShm {
     int red;
     int cur;
     int ws[32];
+    int lp[LB_CELLS];   // sub-block pointers (local indices)
+    int tgt[LB_CELLS];  // sub-block cells' receivers (tile indices)
 };
 
 __device__ __forceinline__ int bceil_log2(long long n)
@@ -191,6 +195,98 @@ __device__ void tile_labels(const Grid &g, int N, const int32_t *rec_, int32_t *
         if (rec_[x] != x) bid[i] = lb[pos[x]];
     }
     __syncthreads();
+}
+
+// ---- labels, fast form for acyclic receivers -----------------------------------------
+//
+// The fixed point of the labelling is bid[i] = root(i)+1, or 0 when the root can leave.
+// Roots are found in three steps: (A) each 32 x 32 sub-block is pointer-jumped in shared
+// memory to its cells' terminals (an in-block root, or the last in-block cell of the
+// path); J[i] = the terminal's receiver, i.e. the root itself or the entry cell of the
+// next sub-block, which lies on that sub-block's perimeter; (B) pointer jumping on J over
+// the perimeter cells only; (C) one gather.  A receiver cycle shows up as a pointer that
+// does not settle or a final target that is not a root; the caller then runs the
+// general labelling, which reproduces the serial result on cycles.
+template <int MODE>
+__device__ bool tile_labels_blocks(const Grid &g, int N, const int32_t *rec_, int32_t *J, int32_t *bid, BatchShm &sh)
+{
+    const int nx = g.nx, ny = g.ny;
+    const int nbx = (nx + LB_SIDE - 1) / LB_SIDE, nby = (ny + LB_SIDE - 1) / LB_SIDE;
+    int bad = 0;
+    // (A) sub-block terminals
+    for (int blk = 0; blk < nbx * nby; ++blk) {
+        const int x0 = (blk % nbx) * LB_SIDE, y0 = (blk / nbx) * LB_SIDE;
+        for (int l = threadIdx.x; l < LB_CELLS; l += blockDim.x) {
+            const int x = x0 + (l & (LB_SIDE - 1)), y = y0 + l / LB_SIDE;
+            int p = l, t = -1;
+            if (x < nx && y < ny) {
+                const int i = y * nx + x;
+                t = rec_[i];
+                const int ry = t / nx, rx = t - ry * nx;
+                if (t != i && rx >= x0 && rx < x0 + LB_SIDE && ry >= y0 && ry < y0 + LB_SIDE)
+                    p = (ry - y0) * LB_SIDE + (rx - x0);
+            }
+            sh.lp[l] = p;
+            sh.tgt[l] = t;
+        }
+        __syncthreads();
+        for (int r = 0; r < 10; ++r) {  // chains inside a block are shorter than 2^10 cells
+            int q[LB_CELLS / 256];      // blockDim >= 256: at most 4 cells per thread
+#pragma unroll
+            for (int c = 0; c < LB_CELLS / 256; ++c) {
+                const int l = threadIdx.x + c * blockDim.x;
+                if (l < LB_CELLS) q[c] = sh.lp[sh.lp[l]];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int c = 0; c < LB_CELLS / 256; ++c) {
+                const int l = threadIdx.x + c * blockDim.x;
+                if (l < LB_CELLS) sh.lp[l] = q[c];
+            }
+            __syncthreads();
+        }
+        for (int l = threadIdx.x; l < LB_CELLS; l += blockDim.x) {
+            const int x = x0 + (l & (LB_SIDE - 1)), y = y0 + l / LB_SIDE;
+            if (x >= nx || y >= ny) continue;
+            const int t = sh.lp[l];
+            if (sh.lp[t] != t) bad = 1;  // a cycle inside the block
+            J[y * nx + x] = sh.tgt[t];
+        }
+        __syncthreads();
+    }
+    if (__syncthreads_or(bad)) return false;
+    // (B) pointer jumping over the perimeter cells (every J value is a root or one of them)
+    const int PER = 4 * LB_SIDE - 4;
+    const int nper = nbx * nby * PER;
+    bool settled = false;
+    for (int r = 0; r < 64; ++r) {
+        int ch = 0;
+        for (int k = threadIdx.x; k < nper; k += blockDim.x) {
+            const int blk = k / PER, e = k - blk * PER;
+            const int x0 = (blk % nbx) * LB_SIDE, y0 = (blk / nbx) * LB_SIDE;
+            const int bw = min(LB_SIDE, nx - x0), bh = min(LB_SIDE, ny - y0);  // the block's extent in the tile
+            int lx, ly;  // position e on the perimeter of the bw x bh block
+            if (e < LB_SIDE) { lx = e; ly = 0; }
+            else if (e < 2 * LB_SIDE) { lx = e - LB_SIDE; ly = bh - 1; }
+            else if (e < 3 * LB_SIDE - 2) { lx = 0; ly = e - 2 * LB_SIDE + 1; }
+            else { lx = bw - 1; ly = e - (3 * LB_SIDE - 2) + 1; }
+            if (lx >= bw || ly >= bh || (e >= 2 * LB_SIDE && ly >= bh - 1)) continue;
+            const int x = x0 + lx, y = y0 + ly;
+            const int i = y * nx + x;
+            const int a = J[i], b2 = J[a];
+            if (b2 != a) { J[i] = b2; ch = 1; }
+        }
+        if (!__syncthreads_or(ch)) { settled = true; break; }
+    }
+    if (!settled) return false;
+    // (C) gather, and check that every target is a true root
+    FOR_CELLS(i, N) {
+        int t = J[i];
+        if (rec_[t] != t) t = J[t];
+        if (rec_[t] != t) { bad = 1; continue; }
+        bid[i] = leave<MODE>(g, t) ? 0 : t + 1;
+    }
+    return !__syncthreads_or(bad);
 }
 
 // ---- saddlesort passes 1-5 (lakeflow.py:106-281) ------------------------------------
@@ -546,7 +642,8 @@ __device__ void tile_reroute(const Grid &g, const BatchTile &T, const BatchArray
         if (it > 0) FOR_CELLS(i, N) nb += (rec_[i] == i && !leave<MODE>(g, i));
         const int nd = it > 0 ? bsum(nb, sh) : ndep;
         if (nd == 0) break;  // (the labels the reference computes first are overwritten)
-        tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
+        if (!tile_labels_blocks<MODE>(g, N, rec_, rec__, bid, sh))
+            tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
         tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
                               A.inv + ob, z);
         tile_carve(N, rec, rec_, A.mark + o, A.tag + o, A.snode + ob, A.outlet + ob, A.status);

@@ -79,7 +79,8 @@ __device__ __forceinline__ void rcv_pick(float zi, const float (&zn)[4], const i
 
 constexpr int RCV_ROWS = 32;
 constexpr int RCV_AHEAD = 4;  // rows loaded per group (RCV_ROWS is a multiple)
-constexpr int RCV4_ROWS = 8;  // rows per warp of the 4-column kernel (a multiple of RCV_AHEAD)
+constexpr int RCV4_ROWS = 8;   // rows per warp of the 4-column kernel
+constexpr int RCV4_AHEAD = 2;  // rows loaded per group there (RCV4_ROWS is a multiple)
 
 template <int MODE>
 __global__ void __launch_bounds__(128) k_receivers(const float *__restrict__ z, int32_t *__restrict__ rcv,
@@ -179,11 +180,60 @@ __device__ __forceinline__ void rcv_pick1(float zi, const float (&zn)[4], const 
     }
 }
 
+// rcv_pick1 for an interior cell, whose four neighbours all exist: k = 0 top (-nx),
+// 1 left (-1), 2 right (+1), 3 bottom (+nx).
+__device__ __forceinline__ void rcv_pick_interior(float zi, float zt, float zl, float zr, float zb, int i, int nx,
+                                                  float dx, int &r, float &sr)
+{
+    const float d0 = __fsub_rn(zi, zt), d1 = __fsub_rn(zi, zl), d2 = __fsub_rn(zi, zr), d3 = __fsub_rn(zi, zb);
+    float dmax = 0.f;
+    dmax = d0 > dmax ? d0 : dmax;
+    dmax = d1 > dmax ? d1 : dmax;
+    dmax = d2 > dmax ? d2 : dmax;
+    dmax = d3 > dmax ? d3 : dmax;
+    if (!(dmax > 0.f)) return;
+    const float q = __fdiv_rn(dmax, dx);
+    if (!(q > 0.f)) return;
+    // the first direction reaching q: an exact maximum, unless an earlier drop ties after
+    // rounding (only possible within a few ulps of dmax: the rare slow path below)
+    const float near = __fmul_rn(dmax, 1.0f - 0x1p-21f);
+    const int first = d0 == dmax ? 0 : d1 == dmax ? 1 : d2 == dmax ? 2 : 3;
+    int k = first;
+    const bool n0 = d0 >= near && first > 0, n1 = d1 >= near && first > 1, n2 = d2 >= near && first > 2;
+    if (n0 | n1 | n2) {
+        if (n0 && __fdiv_rn(d0, dx) == q) k = 0;
+        else if (n1 && __fdiv_rn(d1, dx) == q) k = 1;
+        else if (n2 && __fdiv_rn(d2, dx) == q) k = 2;
+    }
+    r = i + (k == 0 ? -nx : k == 1 ? -1 : k == 2 ? 1 : nx);
+    sr = q;
+}
+
+// A cell on the grid's edge (or any cell in custom mode): neighbours through the
+// boundary rules.  Out of line, so that the interior path keeps its registers.
+template <int MODE>
+__device__ __noinline__ void rcv_boundary(const float *__restrict__ z, const Grid &g, int i, int row, int col, float dx,
+                                          int *r, float *sr)
+{
+    int jn[4];
+    float zn[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        jn[m] = neighbour<MODE>(g, i, row, col, m);
+        zn[m] = jn[m] != -1 ? __ldg(z + jn[m]) : 0.f;
+    }
+    int rr = i;
+    float s = 0.f;
+    rcv_pick1(__ldg(z + i), zn, jn, dx, rr, s);
+    *r = rr;
+    *sr = s;
+}
+
 // Four columns per thread: a warp covers a 128-column strip, rows in groups of
 // RCV_AHEAD; float4 loads and int4 / float4 stores; left and right neighbours from
 // the adjacent lanes.  Needs nx % 4 == 0 (16-byte aligned rows).
 template <int MODE>
-__global__ void __launch_bounds__(128) k_receivers4(const float *__restrict__ z, int32_t *__restrict__ rcv,
+__global__ void __launch_bounds__(128, 6) k_receivers4(const float *__restrict__ z, int32_t *__restrict__ rcv,
                                                     float *__restrict__ grad, Grid g, float dx)
 {
     const int lane = threadIdx.x & 31;
@@ -206,18 +256,18 @@ __global__ void __launch_bounds__(128) k_receivers4(const float *__restrict__ z,
     }
     const bool hl = lane == 0 && c0 > 0 && incol;                         // left halo from memory
     const bool hr = (lane == 31 || c0 + 4 >= nx) && c0 + 4 < nx && incol;  // right halo from memory
-    for (int row = row0; row < row1; row += RCV_AHEAD) {
-        float4 zq[RCV_AHEAD];
-        float ql[RCV_AHEAD], qr[RCV_AHEAD];
+    for (int row = row0; row < row1; row += RCV4_AHEAD) {
+        float4 zq[RCV4_AHEAD];
+        float ql[RCV4_AHEAD], qr[RCV4_AHEAD];
 #pragma unroll
-        for (int q = 0; q < RCV_AHEAD; ++q) {
+        for (int q = 0; q < RCV4_AHEAD; ++q) {
             const int rb = row + 1 + q, rc = row + q;
             zq[q] = (incol && rb < ny && rb <= row1) ? __ldg(z4 + (size_t)rb * nx4 + q0) : make_float4(0.f, 0.f, 0.f, 0.f);
             ql[q] = (hl && rc < row1) ? __ldg(z + (size_t)rc * nx + c0 - 1) : 0.f;
             qr[q] = (hr && rc < row1) ? __ldg(z + (size_t)rc * nx + c0 + 4) : 0.f;
         }
 #pragma unroll
-        for (int q = 0; q < RCV_AHEAD; ++q) {
+        for (int q = 0; q < RCV4_AHEAD; ++q) {
             const int rw = row + q;
             if (rw >= row1) break;
             const float4 zb = zq[q];
@@ -239,18 +289,10 @@ __global__ void __launch_bounds__(128) k_receivers4(const float *__restrict__ z,
                     int r = i;
                     float sr = 0.f;
                     if (rowin && col > 0 && col < nx - 1) {
-                        const float zn[4] = {az[k], k > 0 ? cz[k - 1] : zl, k < 3 ? cz[k + 1] : zr, bz[k]};
-                        const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
-                        rcv_pick1(cz[k], zn, jn, dx, r, sr);
+                        rcv_pick_interior(cz[k], az[k], k > 0 ? cz[k - 1] : zl, k < 3 ? cz[k + 1] : zr, bz[k], i, nx,
+                                          dx, r, sr);
                     } else {
-                        int jn[4];
-                        float zn[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) {
-                            jn[m] = neighbour<MODE>(g, i, rw, col, m);
-                            zn[m] = jn[m] != -1 ? __ldg(z + jn[m]) : 0.f;
-                        }
-                        rcv_pick1(cz[k], zn, jn, dx, r, sr);
+                        rcv_boundary<MODE>(z, g, i, rw, col, dx, &r, &sr);
                     }
                     rr[k] = r;
                     ss[k] = sr;

@@ -292,10 +292,18 @@ __device__ bool tile_labels_blocks(const Grid &g, int N, const int32_t *rec_, in
 // ---- saddlesort passes 1-5 (lakeflow.py:106-281) ------------------------------------
 template <int MODE>
 __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_t *isb, float *zp, long long *sad,
-                                int32_t *snode, long long *out, uint8_t *inv, const float *z)
+                                int32_t *snode, long long *out, uint8_t *inv, const float *z, const int32_t *pl,
+                                int np)
 {
+    // With labels of acyclic receivers (pl given) the only basin ids are 0 and pit + 1 for
+    // the current pits (pl, np entries): those entries are reset and the per-basin passes
+    // run over the pit list.  Otherwise (labels of a receiver cycle, pl == nullptr) every
+    // basin id 0..N is reset and scanned, as in the reference.  Basin N is skipped by the
+    // per-basin passes, as the reference's loops over b < N skip it.
     const long long iv = inv_key();
-    FOR_CELLS(b, N + 1) {
+    const int ninit = pl ? np + 1 : N + 1, nscan = pl ? np : N;
+    for (int k = threadIdx.x; k < ninit; k += blockDim.x) {
+        const int b = pl ? (k < np ? pl[k] + 1 : 0) : k;
         sad[b] = iv;
         out[b] = iv;
         snode[b] = -1;
@@ -359,8 +367,9 @@ __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_
     }
     __syncthreads();
     // pass 4: outlet = lowest foreign neighbour of the saddle node (first k wins)
-    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x) {
-        if (sad[b] == iv) continue;
+    for (int k0 = threadIdx.x; k0 < nscan; k0 += blockDim.x) {
+        const int b = pl ? pl[k0] + 1 : k0;
+        if (b == 0 || b >= N || sad[b] == iv) continue;
         const int node = snode[b];
         if (node < 0) continue;
         float tz = 1e9f;
@@ -380,7 +389,9 @@ __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_
     __syncthreads();
     // pass 5: 2-cycles b -> b' -> b with b' < b, snapshot reads, plus the one basin
     // (bid[42]) whose serial outcome can differ from the snapshot
-    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x) {
+    for (int k0 = threadIdx.x; k0 < nscan; k0 += blockDim.x) {
+        const int b = pl ? pl[k0] + 1 : k0;
+        if (b == 0 || b >= N) continue;
         const long long ob = out[b];
         if (ob == iv) continue;
         const int bd1 = bid[key_index(ob)];
@@ -398,12 +409,14 @@ __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_
         }
     }
     __syncthreads();
-    for (int b = 1 + threadIdx.x; b < N; b += blockDim.x)
-        if (inv[b]) {
+    for (int k0 = threadIdx.x; k0 < nscan; k0 += blockDim.x) {
+        const int b = pl ? pl[k0] + 1 : k0;
+        if (b < N && inv[b]) {
             out[b] = iv;
             sad[b] = iv;
             snode[b] = -1;
         }
+    }
     __syncthreads();
 }
 
@@ -417,7 +430,7 @@ __device__ void tile_saddlesort(const Grid &g, int N, const int32_t *bid, uint8_
 // orbit, stopping at a cell already tagged (the rest of that orbit is another
 // walker's) or at a root.
 __device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *claim, uint8_t *tag, const int32_t *snode,
-                           const long long *out, int *status)
+                           const long long *out, const int32_t *pl, int np, int *status)
 {
     const long long iv = inv_key();
     FOR_CELLS(i, N) {
@@ -426,7 +439,10 @@ __device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *claim, u
     }
     __syncthreads();
     int overrun = 0;
-    FOR_CELLS(b, N) {
+    const int nscan = pl ? np : N;  // the pits' basins, or every basin id (see tile_saddlesort)
+    for (int k0 = threadIdx.x; k0 < nscan; k0 += blockDim.x) {
+        const int b = pl ? pl[k0] + 1 : k0;
+        if (b >= N) continue;
         int x = snode[b];
         if (x == -1) continue;
         int s = 0;
@@ -452,7 +468,9 @@ __device__ void tile_carve(int N, int32_t *rec, int32_t *rec_, int32_t *claim, u
         if (c >= 0) rec[x] = c;
     }
     __syncthreads();
-    FOR_CELLS(b, N) {
+    for (int k0 = threadIdx.x; k0 < nscan; k0 += blockDim.x) {
+        const int b = pl ? pl[k0] + 1 : k0;
+        if (b >= N) continue;
         const long long ob = out[b];
         if (ob != iv) rec[snode[b]] = key_index(ob);
     }
@@ -632,21 +650,32 @@ __device__ void tile_reroute(const Grid &g, const BatchTile &T, const BatchArray
     const long long o = T.off, ob = T.boff;
     int32_t *rec = A.rcv + o, *rec_ = A.rec_ + o, *rec__ = A.rec__ + o, *bid = A.bid + o;
     const int lrounds = bceil_log2(N) + 1;
-    int np = 0;
-    FOR_CELLS(i, N) np += (rec_[i] == i && !leave<MODE>(g, i));
-    const int ndep = bsum(np, sh);
+    int32_t *pl = A.ndnr + o;  // pit list (scratch of the accumulation / diffusion, free here)
+    auto list_pits = [&]() {   // depression_counter (lakeflow.py:25-44), as an ascending list
+        int n = 0;
+        for (int b0 = 0; b0 < N; b0 += blockDim.x) {
+            const int i = b0 + threadIdx.x;
+            const int f = (i < N && rec_[i] == i && !leave<MODE>(g, i)) ? 1 : 0;
+            int tot;
+            const int q = bscan(f, sh, &tot);
+            if (f) pl[n + q] = i;
+            n += tot;
+        }
+        __syncthreads();
+        return n;
+    };
+    const int ndep = list_pits();
     if (ndep == 0) return;
     const int outer = bceil_log2(ndep) + 1;
     for (int it = 0; it < outer; ++it) {
-        int nb = 0;
-        if (it > 0) FOR_CELLS(i, N) nb += (rec_[i] == i && !leave<MODE>(g, i));
-        const int nd = it > 0 ? bsum(nb, sh) : ndep;
+        const int nd = it > 0 ? list_pits() : ndep;
         if (nd == 0) break;  // (the labels the reference computes first are overwritten)
-        if (!tile_labels_blocks<MODE>(g, N, rec_, rec__, bid, sh))
-            tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
+        const bool acyclic = tile_labels_blocks<MODE>(g, N, rec_, rec__, bid, sh);
+        if (!acyclic) tile_labels<MODE>(g, N, rec_, rec__, bid, A.mark + o, A.dnr + 4 * o, lrounds, sh, A.status);
+        const int32_t *bl = acyclic ? pl : nullptr;  // basin ids: the pits', or any (labels of a cycle)
         tile_saddlesort<MODE>(g, N, bid, A.isb + o, A.zp + o, A.saddle + ob, A.snode + ob, A.outlet + ob,
-                              A.inv + ob, z);
-        tile_carve(N, rec, rec_, A.mark + o, A.tag + o, A.snode + ob, A.outlet + ob, A.status);
+                              A.inv + ob, z, bl, nd);
+        tile_carve(N, rec, rec_, A.mark + o, A.tag + o, A.snode + ob, A.outlet + ob, bl, nd, A.status);
     }
 }
 

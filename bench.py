@@ -267,6 +267,13 @@ def main():
     roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
                 "peak_source": pk_kind, "traffic": None,
                 "alg_bytes_per_cell": ALG_BYTES[dom], "stage_ms": st_ms}
+    # the stencil stage (one kernel: receivers), 12 algorithmic bytes per cell
+    ach_s = ALG_BYTES["receivers"] * n * n / (st_ms["receivers"] * 1e-3) / 1e9
+    roofline_stencil = {"bound": "hbm", "kernel": "receivers", "achieved": ach_s, "peak": pk, "unit": "GB/s",
+                        "frac": ach_s / pk, "peak_source": pk_kind, "alg_bytes_per_cell": ALG_BYTES["receivers"],
+                        "traffic": 146e6 * (n * n) / 16777216.0,
+                        "traffic_note": "DRAM read+write of one 4096^2 launch from an ncu capture (67 + 79 MB), "
+                                        "scaled by cells"}
 
     # ---- e2e through the public API with host buffers ----
     zh = torch.from_numpy(z.ravel()).pin_memory()
@@ -299,7 +306,8 @@ def main():
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded spectral DEM + Gaussian pits)",
            "config": dict(cfg, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                           n_outer_reroute=router.last_n_outer),
-           "roofline": roofline, "clocks": clk.summary(), "gpu_launches": int(launches),
+           "roofline": roofline, "roofline_stencil": roofline_stencil, "clocks": clk.summary(),
+           "gpu_launches": int(launches),
            "e2e": {"value": e2e_v, "unit": "Mcells/s", "h2d_bytes_per_step": 8 * n * n,
                    "d2h_bytes_per_step": 8 * n * n, "steps": e2e_steps,
                    "api": "FlowRouter.route_many (copies of neighbouring steps overlap the routing)"}}

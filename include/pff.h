@@ -131,6 +131,14 @@ int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_t *receiver
                          int32_t *receivers_, int32_t *receivers__, double epsilon, int N,
                          void *workspace, size_t workspace_bytes, void *stream);
 
+/* pyfastflow/flow/fill_topo.py:48-78 topofill(flow_field, epsilon, custom_z): the
+ * same rounds on z with increments float(2^it * epsilon), it = 0..ceil(log2 N)-1,
+ * into z_ (snapshot semantics as above); write_back = 1 then copies z_ into z (the
+ * reference's default), 0 leaves z untouched (its custom_z form, z_ = custom_z).
+ * No depth update.  workspace: pff_fill_workspace_bytes(N) bytes. */
+int pff_topofill(float *z, float *z_, const int32_t *receivers, int32_t *receivers_, int32_t *receivers__,
+                 double epsilon, int N, int write_back, void *workspace, size_t workspace_bytes, void *stream);
+
 /* The same fill for callers that cannot allocate device memory (no workspace
  * argument): its scratch is a 16 MiB device array built into the library,
  * held on every GPU that loads the library until exit.  No counterpart in the
@@ -171,7 +179,7 @@ int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, cons
 int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *stream);
 
 /* ---- Ragged batch ----------------------------------------------------------------
- * Many independent tiles (own nx, ny, dx, boundary mode 0-2) packed back to back,
+ * Many independent tiles (own nx, ny, dx, boundary mode 0-3) packed back to back,
  * tile t's cells at [tile_offset[t], tile_offset[t] + nx*ny) in row-major order.
  * One persistent launch runs, per tile, the chain a FlowRouter user runs tile by
  * tile: compute_receivers (receivers.py:16-58), reroute_flow(carve=True)
@@ -185,18 +193,20 @@ int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *
  * uploads the tile table into the workspace (synchronizes `stream`).  Errors are
  * returned negated (-PFF_ERR_*).
  * pff_batch_route: asynchronous launch on `stream`, no host synchronisation, so it
- * can be captured in a CUDA graph.  Q: per-cell seed in, upstream sum out.
+ * can be captured in a CUDA graph.  Q: per-cell seed in, upstream sum out.  codes:
+ * packed uint8 boundary codes (N per tile, read for custom-mode tiles only; NULL if
+ * the batch has none).
  * threads: 256, 512 or 1024 per CTA; ctas_per_sm is clamped to the occupancy.
  * pff_batch_status: error bits of the last launch (synchronizes `stream`):
- * 1 = a tile mode outside 0-2, 8 = cells of one receiver cycle ended with
+ * 1 = a bad tile mode (or a custom-mode tile without codes), 8 = cells of one receiver cycle ended with
  * different serial labels, 16 = a carve did not converge. */
 size_t pff_batch_workspace_bytes(long long total_cells, int ntiles);
 long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_ny, const int32_t *tile_mode,
                          const float *tile_dx, int ntiles, long long *tile_offset, int32_t *order,
                          void *workspace, size_t workspace_bytes, void *stream);
-int pff_batch_route(const float *z, int32_t *receivers, float *gradient, float *Q, uint32_t *counts,
-                    long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
-                    size_t workspace_bytes, void *stream);
+int pff_batch_route(const float *z, const uint8_t *codes, int32_t *receivers, float *gradient, float *Q,
+                    uint32_t *counts, long long total_cells, int ntiles, int threads, int ctas_per_sm,
+                    void *workspace, size_t workspace_bytes, void *stream);
 int pff_batch_status(long long total_cells, int ntiles, void *workspace, size_t workspace_bytes,
                      int *status, void *stream);
 
@@ -211,7 +221,8 @@ int pff_batch_status(long long total_cells, int ntiles, void *workspace, size_t 
  * -1 never.  Per tile (caller order): iters = iterations run, residuals = the last
  * (max|dh|, mean|dh|); trace (optional): niter x (max, mean) per tile.  The mean is
  * summed in an unspecified order.  Asynchronous; status bits as pff_batch_status. */
-int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts, float edgesw, float dt,
+int pff_batch_graphflood(float *zh, const uint8_t *codes, float *h, float *Q, const float *tile_consts,
+                         float edgesw, float dt,
                          int niter, int crit, int32_t *iters, float *residuals, float *trace,
                          long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
                          size_t workspace_bytes, void *stream);

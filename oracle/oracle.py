@@ -256,6 +256,25 @@ def fill_z_add_delta(zh, h, rec, eps: float = 1e-3, serial: bool = False):
     return zh, h, z_
 
 
+def topofill(z, rec, eps: float = 1e-6, serial: bool = False):
+    """fill_topo.topofill (fill_topo.py:48-78 with _topofill :17-45): the same rounds as
+    fill_z_add_delta with increments float32(2**it * eps), it = 0..ceil(log2 N)-1
+    (the reference passes iteration it+1 and adds 2**(iteration-1) * eps); returns the
+    filled surface z_."""
+    z = np.array(z, np.float32, copy=True).ravel()
+    N = z.size
+    inc = np.array([np.float32(2.0 ** it * eps) for it in range(ceil_log2(N))], np.float32)
+    h = np.zeros(N, np.float32)
+    z_ = np.empty(N, np.float32)
+    r_ = np.empty(N, np.int32)
+    r__ = np.empty(N, np.int32)
+    tmp = np.empty(N, np.float32)
+    rec = np.ascontiguousarray(rec, np.int32)
+    lib().orc_fill_z_add_delta_f32(_p(z), _p(h), _p(z_), _p(rec), _p(r_), _p(r__), _p(inc), inc.size, N,
+                                   int(serial), _p(tmp))
+    return z_
+
+
 def diffuse_q(zh, Q, g: Grid, dx: float, prec: float):
     temp = np.empty_like(Q)
     lib().orc_diffuse_q_f32(_p(zh), _p(Q), _p(temp), g.ref, float(np.float32(dx)),

@@ -36,16 +36,17 @@ SIGNATURES = {
     "pff_fill_workspace_bytes": (_sz, [_i32]),
     "pff_fill_z_add_delta": (_i32, [_vp] * 6 + [_f64, _i32, _vp, _sz, _vp]),
     "pff_fill_z_add_delta_noalloc": (_i32, [_vp] * 6 + [_f64, _i32, _vp]),
+    "pff_topofill": (_i32, [_vp] * 5 + [_f64, _i32, _i32, _vp, _sz, _vp]),
     "pff_diffuse_workspace_bytes": (_sz, [_i32]),
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
     "pff_abs_diff_stats": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "pff_batch_workspace_bytes": (_sz, [_i64, _i32]),
     "pff_batch_plan": (_i64, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
-    "pff_batch_route": (_i32, [_vp] * 5 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),
+    "pff_batch_route": (_i32, [_vp] * 6 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),
     "pff_batch_status": (_i32, [_i64, _i32, _vp, _sz, C.POINTER(C.c_int), _vp]),
-    "pff_batch_graphflood": (_i32, [_vp, _vp, _vp, _vp, _f32, _f32, _i32, _i32, _vp, _vp, _vp, _i64, _i32, _i32,
-                                    _i32, _vp, _sz, _vp]),
+    "pff_batch_graphflood": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _i32, _i32, _vp, _vp, _vp, _i64, _i32,
+                                    _i32, _i32, _vp, _sz, _vp]),
     "pff_conv3x3_fwd": (_i32, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32] + [_i32] * 7 + [_vp]),
     "pff_conv_set_path": (_i32, [_i32]),
     "pff_conv_tc_status": (_i32, [C.POINTER(C.c_int)]),

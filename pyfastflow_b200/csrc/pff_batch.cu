@@ -28,6 +28,7 @@ struct BatchTile {
 // Packed per-cell and per-basin arrays of the batch (device pointers).
 struct BatchArrays {
     const float *z;
+    const uint8_t *codes;  // packed boundary codes of the custom-mode tiles (may be null without such tiles)
     int32_t *rcv;      // out: rerouted receivers (tile-local indices)
     float *grad;       // out: steepest gradient of the original receivers
     float *Q;          // in: per-cell seed, out: upstream sum
@@ -682,7 +683,7 @@ __device__ void tile_reroute(const Grid &g, const BatchTile &T, const BatchArray
 template <int MODE>
 __device__ void route_tile(const BatchTile &T, const BatchArrays &A, BatchShm &sh)
 {
-    const Grid g{T.nx, T.ny, MODE, nullptr};
+    const Grid g{T.nx, T.ny, MODE, MODE == 3 ? A.codes + T.off : nullptr};
     const int N = T.nx * T.ny;
     const long long o = T.off;
     const float *z = A.z + o;
@@ -734,7 +735,7 @@ __device__ __forceinline__ void bmaxsum(float m, float sum, BatchShm &sh, float 
 template <int MODE>
 __device__ void gf_tile(const BatchTile &T, const BatchArrays &A, const GfParams &P, BatchShm &sh)
 {
-    const Grid g{T.nx, T.ny, MODE, nullptr};
+    const Grid g{T.nx, T.ny, MODE, MODE == 3 ? A.codes + T.off : nullptr};
     const int N = T.nx * T.ny;
     const long long o = T.off;
     float *zh = const_cast<float *>(A.z) + o, *h = P.h + o, *Q = A.Q + o;
@@ -809,7 +810,7 @@ __device__ void gf_tile(const BatchTile &T, const BatchArrays &A, const GfParams
             FOR_CELLS(j, N) {
                 const int row = j / g.nx, col = j - row * g.nx;
                 float acc = prec_dx2;
-                if (row > 0 && row < g.ny - 1 && col > 0 && col < g.nx - 1) {
+                if (MODE != 3 && row > 0 && row < g.ny - 1 && col > 0 && col < g.nx - 1) {
                     const int nx = g.nx;
                     if (issrc[j - nx]) acc = __fadd_rn(acc, __fmul_rn(w[3 * (size_t)N + j - nx], qa[j - nx]));
                     if (issrc[j - 1]) acc = __fadd_rn(acc, __fmul_rn(w[2 * (size_t)N + j - 1], qa[j - 1]));
@@ -893,6 +894,10 @@ __global__ void __launch_bounds__(1024) k_batch_route(int ntiles, BatchArrays A)
         case 0: route_tile<0>(T, A, sh); break;
         case 1: route_tile<1>(T, A, sh); break;
         case 2: route_tile<2>(T, A, sh); break;
+        case 3:
+            if (A.codes) route_tile<3>(T, A, sh);
+            else if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
+            break;
         default:
             if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
             break;
@@ -916,6 +921,10 @@ __global__ void __launch_bounds__(1024) k_batch_graphflood(int ntiles, BatchArra
         case 0: gf_tile<0>(T, A, P, sh); break;
         case 1: gf_tile<1>(T, A, P, sh); break;
         case 2: gf_tile<2>(T, A, P, sh); break;
+        case 3:
+            if (A.codes) gf_tile<3>(T, A, P, sh);
+            else if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
+            break;
         default:
             if (threadIdx.x == 0) atomicOr(A.status, BST_MODE);
             break;
@@ -1012,9 +1021,9 @@ extern "C" long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_
     long long off = 0;
     for (int t = 0; t < ntiles; ++t) {
         const int nx = tile_nx[t], ny = tile_ny[t], md = tile_mode[t];
-        if (nx < 2 || ny < 2 || md < 0 || md > 2 || (long long)nx * ny * 4 >= (1LL << 31) ||
+        if (nx < 2 || ny < 2 || md < 0 || md > 3 || (long long)nx * ny * 4 >= (1LL << 31) ||
             !(tile_dx[t] > 0.f)) {
-            set_error("pff_batch_plan: tile %d: bad size %dx%d, mode %d or dx (modes 0-2 are batched)", t, nx, ny,
+            set_error("pff_batch_plan: tile %d: bad size %dx%d, mode %d or dx (modes 0-3)", t, nx, ny,
                       md);
             return -PFF_ERR_ARG;
         }
@@ -1049,9 +1058,9 @@ extern "C" long long pff_batch_plan(const int32_t *tile_nx, const int32_t *tile_
     return total;
 }
 
-extern "C" int pff_batch_route(const float *z, int32_t *receivers, float *gradient, float *Q, uint32_t *counts,
-                               long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
-                               size_t workspace_bytes, void *stream)
+extern "C" int pff_batch_route(const float *z, const uint8_t *codes, int32_t *receivers, float *gradient, float *Q,
+                               uint32_t *counts, long long total_cells, int ntiles, int threads, int ctas_per_sm,
+                               void *workspace, size_t workspace_bytes, void *stream)
 {
     clear_error();
     PFF_TRY(batch_check(total_cells, ntiles, workspace, workspace_bytes, "pff_batch_route"));
@@ -1072,6 +1081,7 @@ extern "C" int pff_batch_route(const float *z, int32_t *receivers, float *gradie
     BatchWs w = carve_batch(workspace, workspace_bytes, total_cells, ntiles);
     BatchArrays A = w.A;
     A.z = z;
+    A.codes = codes;
     A.rcv = receivers;
     A.grad = gradient;
     A.Q = Q;
@@ -1099,7 +1109,8 @@ extern "C" int pff_batch_status(long long total_cells, int ntiles, void *workspa
     return PFF_OK;
 }
 
-extern "C" int pff_batch_graphflood(float *zh, float *h, float *Q, const float *tile_consts, float edgesw, float dt,
+extern "C" int pff_batch_graphflood(float *zh, const uint8_t *codes, float *h, float *Q, const float *tile_consts,
+                                    float edgesw, float dt,
                                     int niter, int crit, int32_t *iters, float *residuals, float *trace,
                                     long long total_cells, int ntiles, int threads, int ctas_per_sm, void *workspace,
                                     size_t workspace_bytes, void *stream)
@@ -1123,6 +1134,7 @@ extern "C" int pff_batch_graphflood(float *zh, float *h, float *Q, const float *
     BatchWs w = carve_batch(workspace, workspace_bytes, total_cells, ntiles);
     BatchArrays A = w.A;
     A.z = zh;
+    A.codes = codes;
     A.Q = Q;
     A.rcv = A.src;  // the rerouted receivers of each iteration (the accumulation arrays are unused)
     A.grad = nullptr;

@@ -301,6 +301,44 @@ extern "C" int pff_fill_z_add_delta_noalloc(float *zh, float *h, float *z_, cons
     return check_cuda("pff_fill_z_add_delta_noalloc");
 }
 
+// topofill (fill_topo.py:48-78 driving _topofill :17-45): the same pointer-jumping
+// rounds with increments 2^it * epsilon for it = 0..ceil(log2 N)-1 (the reference
+// passes iteration it+1 and uses 2^(iteration-1)), then z = z_; no depth update.
+extern "C" int pff_topofill(float *z, float *z_, const int32_t *receivers, int32_t *receivers_, int32_t *receivers__,
+                            double epsilon, int N, int write_back, void *workspace, size_t workspace_bytes,
+                            void *stream)
+{
+    clear_error();
+    if (N <= 1 || !z || !z_ || !receivers || !receivers_ || !receivers__) {
+        set_error("pff_topofill: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    if (!workspace || workspace_bytes < pff_fill_workspace_bytes(N)) {
+        set_error("pff_topofill: workspace too small");
+        return PFF_ERR_WORKSPACE;
+    }
+    cudaStream_t st = S(stream);
+    Carver cv(workspace, workspace_bytes);
+    float *zt = cv.take<float>(N);
+    const size_t nbf = sizeof(float) * (size_t)N, nbi = sizeof(int32_t) * (size_t)N;
+    PFF_CUDA(cudaMemcpyAsync(z_, z, nbf, cudaMemcpyDeviceToDevice, st));
+    PFF_CUDA(cudaMemcpyAsync(receivers_, receivers, nbi, cudaMemcpyDeviceToDevice, st));
+    int nr = 0;
+    for (long long p = 1; p < N; p <<= 1) ++nr;
+    float *zs = z_, *zn = zt;
+    int32_t *ra = receivers_, *rb = receivers__;
+    for (int it = 0; it < nr; ++it) {
+        const float inc = (float)(ldexp(1.0, it) * epsilon);  // = 2^it * float(epsilon): a power-of-2 scaling
+        { k_fill_round<<<div_up(N, 256), 256, 0, st>>>(z, zs, zn, ra, rb, inc, N); count_launch(); }
+        float *tz = zs; zs = zn; zn = tz;
+        int32_t *tr = ra; ra = rb; rb = tr;
+    }
+    if (zs != z_) PFF_CUDA(cudaMemcpyAsync(z_, zs, nbf, cudaMemcpyDeviceToDevice, st));
+    PFF_CUDA(cudaMemcpyAsync(rb, ra, nbi, cudaMemcpyDeviceToDevice, st));
+    if (write_back) PFF_CUDA(cudaMemcpyAsync(z, z_, nbf, cudaMemcpyDeviceToDevice, st));
+    return check_cuda("pff_topofill");
+}
+
 extern "C" size_t pff_diffuse_workspace_bytes(int N)
 {
     return Carver::round(sizeof(float) * 4 * (size_t)N) + Carver::round((size_t)N) + 512;

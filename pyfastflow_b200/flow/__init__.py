@@ -9,7 +9,7 @@ from .receivers import compute_receivers
 from .downstream_propag import rcv2donor, rake_compress_accum, fuse
 from .lakeflow import depression_counter, basin_identification, saddlesort, reroute_flow
 from .f32_i32_struct import pack_float_index, unpack_float_index
-from .fill_topo import fill_z_add_delta
+from .fill_topo import fill_z_add_delta, topofill
 from .flowfields import FlowRouter
 from .ragged import RaggedRouter
 from . import environment, receivers, downstream_propag, lakeflow, f32_i32_struct, fill_topo, flowfields, ragged
@@ -18,6 +18,6 @@ __all__ = [
     "environment", "receivers", "downstream_propag", "lakeflow", "f32_i32_struct", "fill_topo", "flowfields",
     "ragged",
     "FlowRouter", "RaggedRouter", "compute_receivers", "rcv2donor", "rake_compress_accum", "fuse", "depression_counter",
-    "basin_identification", "saddlesort", "reroute_flow", "fill_z_add_delta", "pack_float_index",
+    "basin_identification", "saddlesort", "reroute_flow", "fill_z_add_delta", "topofill", "pack_float_index",
     "unpack_float_index", "initialise", "reboot",
 ]

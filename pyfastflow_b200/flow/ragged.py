@@ -2,8 +2,9 @@
 
 The reference routes one grid per process (its grid size is a module global,
 pyfastflow/constants.py).  ``RaggedRouter`` holds many tiles of their own shape,
-cell size and boundary mode (0 normal, 1 periodic E-W, 2 periodic N-S) packed back
-to back, and runs for every tile the chain a ``FlowRouter`` user runs tile by tile:
+cell size and boundary mode (0 normal, 1 periodic E-W, 2 periodic N-S, 3 custom
+codes) packed back to back, and runs for every tile the chain a ``FlowRouter``
+user runs tile by tile:
 
     compute_receivers()                 (flow/receivers.py:16-58)
     reroute_flow(carve=True)            (flow/lakeflow.py:466-538)
@@ -32,15 +33,17 @@ def _mode_code(m) -> int:
     if isinstance(m, str):
         m = BOUND_MODES[m]
     m = int(m)
-    if m not in (0, 1, 2):
-        raise ValueError(f"ragged tiles take boundary modes 0-2 (normal, periodic_EW, periodic_NS), got {m}")
+    if m not in (0, 1, 2, 3):
+        raise ValueError(f"boundary modes are 0-3 (normal, periodic_EW, periodic_NS, custom), got {m}")
     return m
 
 
 class RaggedRouter:
-    """A packed batch of tiles; ``shapes`` is a list of (ny, nx)."""
+    """A packed batch of tiles; ``shapes`` is a list of (ny, nx).  Custom-mode tiles
+    ("custom" / 3) take their uint8 boundary codes (ny, nx) from ``codes``, a list
+    with None for the other tiles (pyfastflow/constants.py:56-83 codes)."""
 
-    def __init__(self, shapes, dx, modes, device=None):
+    def __init__(self, shapes, dx, modes, codes=None, device=None):
         self.ntiles = len(shapes)
         if self.ntiles == 0:
             raise ValueError("empty batch")
@@ -69,6 +72,20 @@ class RaggedRouter:
         if total != self.total:
             raise _lib.PFFError(f"pff_batch_plan failed with status {-total}: "
                                 f"{lib.pff_last_error_string().decode(errors='replace')}")
+        self.codes = None
+        if (self.mode == 3).any():
+            if codes is None or len(codes) != self.ntiles:
+                raise ValueError("custom-mode tiles need a codes list (one entry per tile, None where unused)")
+            packed = np.zeros(self.total, np.uint8)
+            for t in range(self.ntiles):
+                if self.mode[t] != 3:
+                    continue
+                c = np.asarray(codes[t], np.uint8)
+                if c.size != self.cells(t):
+                    raise ValueError(f"tile {t}: {c.size} codes for {self.cells(t)} cells")
+                o = int(self.offset[t])
+                packed[o:o + c.size] = c.ravel()
+            self.codes = torch.from_numpy(packed).to(self.device)
         T = lambda dt: torch.zeros(self.total, dtype=dt, device=self.device)  # noqa: E731
         self.z = T(torch.float32)
         self.receivers = T(torch.int32)
@@ -132,7 +149,8 @@ class RaggedRouter:
     # ---- routing ------------------------------------------------------------------------
     def _launch(self, threads: int, ctas: int):
         self.Q.copy_(self.seed)
-        _lib.call("pff_batch_route", self.z.data_ptr(), self.receivers.data_ptr(), self.gradient.data_ptr(),
+        _lib.call("pff_batch_route", self.z.data_ptr(), self.codes.data_ptr() if self.codes is not None else None,
+                  self.receivers.data_ptr(), self.gradient.data_ptr(),
                   self.Q.data_ptr(), self.counts.data_ptr(), self.total, self.ntiles, threads, ctas,
                   self.ws.data_ptr(), self.ws_bytes, _dev.stream())
 

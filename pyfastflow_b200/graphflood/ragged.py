@@ -47,7 +47,8 @@ class RaggedFlooder:
         r = self.router
         cst = self._consts(tol_ratio)
         tr = torch.zeros(r.ntiles * max(niter, 1) * 2, dtype=torch.float32, device=r.device) if trace else None
-        _lib.call("pff_batch_graphflood", r.z.data_ptr(), self.h.data_ptr(), r.Q.data_ptr(), cst.data_ptr(),
+        _lib.call("pff_batch_graphflood", r.z.data_ptr(), r.codes.data_ptr() if r.codes is not None else None,
+                  self.h.data_ptr(), r.Q.data_ptr(), cst.data_ptr(),
                   float(np.float32(self.edge_slope)), float(np.float32(cte.DT_HYDRO)), int(niter), STOP[stop],
                   self.iters.data_ptr(), self.residuals.data_ptr(), tr.data_ptr() if trace else None, r.total,
                   r.ntiles, threads, ctas_per_sm, r.ws.data_ptr(), r.ws_bytes, _dev.stream())

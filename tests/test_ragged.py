@@ -61,8 +61,10 @@ def test_plan_offsets_and_errors():
     assert tot == 20 + 14 + 27
     assert off.tolist() == [0, 20, 34]
     assert lib.pff_batch_workspace_bytes(tot, 3) > 100 * tot
-    tot, _, _ = _plan(lib, [5, 7], [4, 2], [0, 3], [1.0, 1.0])  # custom codes are not batched
-    assert tot == -1 and b"mode 3" in lib.pff_last_error_string()
+    tot, _, _ = _plan(lib, [5, 7], [4, 2], [0, 3], [1.0, 1.0])  # custom codes are batched too
+    assert tot == 34
+    tot, _, _ = _plan(lib, [5, 7], [4, 2], [0, 4], [1.0, 1.0])
+    assert tot == -1 and b"mode 4" in lib.pff_last_error_string()
     tot, _, _ = _plan(lib, [1, 7], [4, 2], [0, 0], [1.0, 1.0])
     assert tot == -1
     tot, _, _ = _plan(lib, [4, 7], [4, 2], [0, 0], [1.0, 0.0])  # dx must be positive
@@ -202,3 +204,62 @@ def test_ragged_graphflood_stops_per_tile(cuda):
             thr = np.float32(1e4 * 1e-5 * 5e-3)
             assert tr[k, n - 1, 1] < thr and (tr[k, :n - 1, 1] >= thr).all()
         assert bits(res[k, 0]) == bits(tr[k, n - 1, 0])  # (a tile whose h went NaN never stops early)
+
+
+def custom_codes(nx, ny, seed):
+    """Boundary codes of a custom-mode tile: outlets (3) on the south row and a few
+    interior outlet cells, nodata (0) holes, periodic (9) west/east columns, inlets (7),
+    normal (1) elsewhere (pyfastflow/constants.py:56-83)."""
+    rng = np.random.default_rng(seed)
+    c = np.ones((ny, nx), np.uint8)
+    c[-1, :] = 3
+    c[:, 0] = 9
+    c[:, -1] = 9
+    c[-1, 0] = c[-1, -1] = 3
+    c[rng.integers(1, ny - 1, 4), rng.integers(1, nx - 1, 4)] = 0
+    c[rng.integers(1, ny - 1, 2), rng.integers(1, nx - 1, 2)] = 3
+    c[0, rng.integers(1, nx - 1, 3)] = 7
+    return c
+
+
+@pytest.mark.gpu
+def test_ragged_custom_codes_bit_exact(orc, cuda):
+    """Custom-mode tiles (codes 0/1/3/7/9) mixed with the other modes, routed and
+    flooded in one launch each, equal the oracle tile by tile."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+
+    tiles = synthetic.ragged_tiles(ntiles=6, seed=41, side_min=24, side_max=96, max_pits=10, dx=10.0)
+    codes = [None] * len(tiles)
+    for k in (1, 3, 4):
+        tiles[k]["mode"] = "custom"
+        codes[k] = custom_codes(tiles[k]["nx"], tiles[k]["ny"], 100 + k)
+    modes = [t["mode"] for t in tiles]
+    rr = pf.flow.RaggedRouter([(t["ny"], t["nx"]) for t in tiles], 10.0, modes, codes=codes)
+    rr.set_z([t["z"] for t in tiles])
+    rr.seed_constant(1.0, area=True)
+    rr.route()
+    torch.cuda.synchronize()
+    code_of = {"normal": 0, "periodic_EW": 1, "periodic_NS": 2, "custom": 3}
+    for k, t in enumerate(tiles):
+        g = orc.Grid(t["nx"], t["ny"], code_of[t["mode"]], codes[k].ravel() if codes[k] is not None else None)
+        rcv, grad = orc.compute_receivers(t["z"], g, t["dx"])
+        r, _, _, _, _ = orc.reroute_flow(rcv, t["z"], g, carve=True)
+        Q, cnt = orc.accumulate(r, np.float32(t["dx"] * t["dx"]))
+        assert np.array_equal(rr.get_receivers(k).ravel(), r), f"tile {k} receivers"
+        assert np.array_equal(rr.get_counts(k).ravel(), cnt), f"tile {k} counts"
+        assert np.array_equal(bits(rr.get_Q(k)), bits(Q)), f"tile {k} Q"
+    # GraphFlood on the same batch
+    rr.set_z([t["z"] for t in tiles])
+    rr.Q.zero_()
+    fl = pf.graphflood.RaggedFlooder(rr, precipitation_rates=2e-5, manning=0.04)
+    fl.run(25, stop=None)
+    torch.cuda.synchronize()
+    for k, t in enumerate(tiles):
+        g = orc.Grid(t["nx"], t["ny"], code_of[t["mode"]], codes[k].ravel() if codes[k] is not None else None)
+        zh = t["z"].ravel().copy()
+        h = np.zeros_like(zh)
+        Q = np.zeros_like(zh)
+        orc.graphflood_run(zh, h, Q, g, 10.0, 2e-5, manning=0.04, niter=25)
+        assert np.array_equal(bits(fl.get_h(k)), bits(h)), f"tile {k} h"
+        assert np.array_equal(bits(rr.Q[int(rr.offset[k]):int(rr.offset[k]) + rr.cells(k)].cpu().numpy()), bits(Q))

@@ -57,6 +57,15 @@ int pff_set_device(int device);
 int pff_compute_receivers(const float *z, int32_t *receivers, float *gradient, int nx, int ny,
                           float dx, int bound_mode, const uint8_t *codes, void *stream);
 
+/* receivers.py:46-47 with RAND_RCV: every direction's slope (or -1 if the neighbour
+ * is invalid) is multiplied by u in [0, 1) before the same strict '>' selection; the
+ * gradient is the chosen scaled slope.  u = (SplitMix64(seed ^ SplitMix64(4*i + k))
+ * >> 40) / 2^24: reproducible for a seed; the reference's draws (Taichi's generator)
+ * are not, so parity is statistical. */
+int pff_compute_receivers_stochastic(const float *z, int32_t *receivers, float *gradient, int nx, int ny,
+                                     float dx, int bound_mode, const uint8_t *codes,
+                                     unsigned long long seed, void *stream);
+
 /* ---- accumulation (rake and compress) ----------------------------------------
  * Kernel-level mirrors of pyfastflow/flow/downstream_propag.py with identical
  * semantics (donor slots in ascending donor index, as the reference's serial

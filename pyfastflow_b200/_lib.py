@@ -22,6 +22,7 @@ SIGNATURES = {
     "pff_launch_count": (C.c_longlong, []),
     "pff_set_device": (_i32, [_i32]),
     "pff_compute_receivers": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, _vp]),
+    "pff_compute_receivers_stochastic": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, C.c_uint64, _vp]),
     "pff_rcv2donor": (_i32, [_vp, _vp, _vp, _i32, _vp]),
     "pff_rake_compress_accum": (_i32, [_vp] * 7 + [_i32, _i32, _vp]),
     "pff_fuse": (_i32, [_vp, _vp, _vp, _i32, _i32, _vp]),

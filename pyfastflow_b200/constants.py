@@ -14,7 +14,8 @@ INITIALISED = False
 DX = 1.0          # cell size (constants.py:28)
 NX = 512          # columns (:31)
 NY = 512          # rows (:34)
-RAND_RCV = False  # stochastic receivers (:37) -- not supported by this implementation
+RAND_RCV = False  # stochastic receivers (:37)
+RAND_SEED = 0  # base seed of the stochastic receivers' counter-based draws (no reference counterpart)
 
 # 0 normal (all edges outlets), 1 periodic east-west, 2 periodic north-south,
 # 3 custom per-cell codes: 0 nodata, 1 normal, 3 outlet, 7 inlet, 9 periodic (:39-50)

@@ -322,9 +322,74 @@ static void launch_receivers(const float *z, int32_t *rcv, float *grad, const Gr
     { k_receivers<MODE><<<div_up(warps, 4), 128, 0, st>>>(z, rcv, grad, g, dx); count_launch(); }
 }
 
+// Stochastic receivers (receivers.py:46-47, RAND_RCV): each direction's slope is scaled
+// by a uniform number in [0, 1) before the strict '>' selection.  The reference draws
+// from Taichi's generator; here u(seed, i, k) is a counter-based draw: SplitMix64
+// (Steele, Lea, Flood 2014) of seed and 4*i + k, top 24 bits / 2^24.
+__host__ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__device__ __forceinline__ float uniform01(unsigned long long seed, long long i, int k)
+{
+    const unsigned long long h = splitmix64(seed ^ splitmix64((unsigned long long)(4 * i + k)));
+    return (float)(h >> 40) * 0x1p-24f;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_receivers_stochastic(const float *__restrict__ z, int32_t *__restrict__ rcv,
+                                                              float *__restrict__ grad, Grid g, float dx,
+                                                              unsigned long long seed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.N()) return;
+    const int row = i / g.nx, col = i - row * g.nx;
+    const float zi = z[i];
+    int r = i;
+    float sr = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j = neighbour<MODE>(g, i, row, col, k);
+        const bool valid = j != -1;
+        float tsr = valid ? __fdiv_rn(__fsub_rn(zi, z[j]), dx) : -1.f;
+        tsr = __fmul_rn(tsr, uniform01(seed, i, k));
+        if (valid && tsr > sr) {
+            sr = tsr;
+            r = j;
+        }
+    }
+    rcv[i] = r;
+    grad[i] = sr;
+}
+
 }  // namespace pff
 
 using namespace pff;
+
+extern "C" int pff_compute_receivers_stochastic(const float *z, int32_t *receivers, float *gradient, int nx, int ny,
+                                                float dx, int bound_mode, const uint8_t *codes,
+                                                unsigned long long seed, void *stream)
+{
+    clear_error();
+    PFF_TRY(check_grid(nx, ny, bound_mode, codes));
+    if (!z || !receivers || !gradient) {
+        set_error("pff_compute_receivers_stochastic: null pointer");
+        return PFF_ERR_ARG;
+    }
+    Grid g{nx, ny, bound_mode, codes};
+    const int N = nx * ny;
+    cudaStream_t st = S(stream);
+    switch (bound_mode) {
+    case 0: { k_receivers_stochastic<0><<<div_up(N, 256), 256, 0, st>>>(z, receivers, gradient, g, dx, seed); count_launch(); } break;
+    case 1: { k_receivers_stochastic<1><<<div_up(N, 256), 256, 0, st>>>(z, receivers, gradient, g, dx, seed); count_launch(); } break;
+    case 2: { k_receivers_stochastic<2><<<div_up(N, 256), 256, 0, st>>>(z, receivers, gradient, g, dx, seed); count_launch(); } break;
+    default: { k_receivers_stochastic<3><<<div_up(N, 256), 256, 0, st>>>(z, receivers, gradient, g, dx, seed); count_launch(); } break;
+    }
+    return check_cuda("pff_compute_receivers_stochastic");
+}
 
 extern "C" int pff_version(void) { return 100; }
 extern "C" const char *pff_last_error_string(void) { return g_err; }

@@ -20,8 +20,6 @@ from .f32_i32_struct import INVALID_KEY
 class FlowRouter:
     def __init__(self, nx, ny, dx, boundary_mode="normal", boundaries=None, lakeflow=True,
                  stochastic_receivers=False, device="cuda"):
-        if stochastic_receivers:
-            raise NotImplementedError("stochastic receivers are not supported")
         if boundary_mode not in cte.BOUND_MODES:
             boundary_mode = "normal"  # the reference falls back to mode 0 (flowfields.py:169-175)
         self.nx, self.ny, self.dx = int(nx), int(ny), float(dx)
@@ -29,7 +27,7 @@ class FlowRouter:
         self.boundary_mode = boundary_mode
         self.mode = cte.BOUND_MODES[boundary_mode]
         self.lakeflow = lakeflow
-        self.stochastic_receivers = False
+        self.stochastic_receivers = bool(stochastic_receivers)
         self.device = torch.device(device)
         N = self.nx * self.ny
         self.N = N
@@ -76,7 +74,7 @@ class FlowRouter:
         self.last_n_outer = 0
         # global configuration, as the reference writes it (flowfields.py:163-182)
         cte.NX, cte.NY, cte.DX = self.nx, self.ny, self.dx
-        cte.RAND_RCV = False
+        cte.RAND_RCV = self.stochastic_receivers  # flowfields.py:166
         cte.BOUND_MODE = self.mode
         if self.mode == 3:
             cte.boundaries = self.codes
@@ -115,8 +113,17 @@ class FlowRouter:
         return self.counts.cpu().numpy().view(np.uint32).reshape(self.rshp)
 
     # ---- pipeline -----------------------------------------------------------------
-    def compute_receivers(self):
-        """flowfields.py:216-226 -> receivers.py:15-58."""
+    def compute_receivers(self, seed=None):
+        """flowfields.py:216-226 -> receivers.py:15-58; stochastic (receivers.py:46-47)
+        if the router was made with stochastic_receivers=True (seed: the draw's seed,
+        default a fresh one per call)."""
+        if self.stochastic_receivers:
+            from .receivers import next_seed
+
+            _lib.call("pff_compute_receivers_stochastic", self.z.data_ptr(), self.receivers.data_ptr(),
+                      self.gradient.data_ptr(), self.nx, self.ny, self.dx, self.mode, self._codes(),
+                      next_seed() if seed is None else int(seed), _dev.stream())
+            return
         _lib.call("pff_compute_receivers", self.z.data_ptr(), self.receivers.data_ptr(), self.gradient.data_ptr(),
                   self.nx, self.ny, self.dx, self.mode, self._codes(), _dev.stream())
 

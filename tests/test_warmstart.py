@@ -28,6 +28,7 @@ def _w_ours(w):  # [Cout][Cin][3][3] -> [Cout][9][Cin]
 
 
 def _rel(a, b):
+    a, b = a.detach(), b.detach()
     return float((a - b).abs().max() / (b.abs().max() + 1e-12))
 
 

@@ -29,6 +29,24 @@ TUNE_CANDIDATES = ((1024, 1), (512, 1), (512, 2), (256, 2), (256, 4), (256, 5))
 _tuned: dict = {}  # batch signature -> (threads, ctas_per_sm)
 
 
+def partition_tiles(cells, world: int):
+    """Split tiles over `world` ranks, largest first onto the least loaded rank
+    (longest-processing-time bin packing; ties go to the lower rank).  Tiles are
+    independent, so the ranks need no collective on the data path.  Returns one
+    ascending list of tile indices per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    cells = [int(c) for c in cells]
+    order = sorted(range(len(cells)), key=lambda t: (-cells[t], t))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for t in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(t)
+        load[r] += cells[t]
+    return [sorted(p) for p in parts]
+
+
 def _mode_code(m) -> int:
     if isinstance(m, str):
         m = BOUND_MODES[m]

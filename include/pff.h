@@ -262,7 +262,7 @@ int pff_batch_graphflood(float *zh, const uint8_t *codes, float *h, float *Q, co
  * pff_unet_features: 8-channel bf16 input rows for B tiles of N cells from the
  *   elevation, steepest slope, drainage counts, per-tile rainfall and Manning n;
  *   stats receives each tile's elevation mean and 1/std (2 floats per tile).
- * pff_unet_h0: h0 = max(exp(pred) - eps, 0), and the water surface zh = z + h0 if zh is
+ * pff_unet_h0: h0 = max(exp(min(pred, 5)) - eps, 0), and the water surface zh = z + h0 if zh is
  *   not NULL; pff_unet_target: log(max(h,0) + eps). */
 int pff_conv3x3_fwd(const uint16_t *x, int csx, int offx, const uint16_t *w, const float *bias, void *y,
                     int csy, int offy, int B, int H, int W, int Cin, int Cout, int relu, int out_f32,

@@ -87,13 +87,15 @@ __global__ void k_unet_features(const float *__restrict__ z, const float *__rest
     }
 }
 
-// h0 = max(exp(pred) - eps, 0) from channel 0 of rows of cs floats; with a bed z, also
+// h0 = max(exp(min(pred, 5)) - eps, 0) from channel 0 of rows of cs floats; with a bed z, also
 // the water surface zh = z + h0 (GraphFlood's state holds the surface, not the bed)
 __global__ void k_unet_h0(const float *__restrict__ pred, int cs, float *h0, long long P, float eps,
                           const float *__restrict__ z, float *zh)
 {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
-        const float h = fmaxf(expf(pred[p * cs]) - eps, 0.f);
+        // the log depth is capped at 5 (148 m): a prediction far outside the training
+        // range must not reach the solver as an overflowing depth
+        const float h = fmaxf(expf(fminf(pred[p * cs], 5.f)) - eps, 0.f);
         h0[p] = h;
         if (zh) zh[p] = __fadd_rn(z[p], h);
     }

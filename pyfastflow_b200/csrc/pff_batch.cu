@@ -767,17 +767,22 @@ __device__ void gf_tile(const BatchTile &T, const BatchArrays &A, const GfParams
         int32_t *pa = ra, *pb = rb;
         for (int r = 0; r < nr; ++r) {
             const float inc = (float)(ldexp(1.0, r - 1) * (double)P.eps);
+            int ch = 0;
             FOR_CELLS(i, N) {
                 const int q = pa[i];
                 const int qq = pa[q];
                 pb[i] = qq;
                 const float zi = a[i];
-                if (i == q || (zi > zh[q] && qq == q)) b[i] = zi;
-                else b[i] = fmaxf(zi, __fadd_rn(a[q], inc));
+                float zo = zi;
+                if (!(i == q || (zi > zh[q] && qq == q))) zo = fmaxf(zi, __fadd_rn(a[q], inc));
+                b[i] = zo;
+                ch |= qq != q || __float_as_uint(zo) != __float_as_uint(zi);
             }
-            __syncthreads();
+            const bool any = __syncthreads_or(ch);
             float *t = a; a = b; b = t;
             int32_t *u = pa; pa = pb; pb = u;
+            // a round that changed nothing is a fixed point of every later round (see k_fill_round)
+            if (!any) break;
         }
         FOR_CELLS(i, N) {
             const float zf = a[i];

@@ -96,6 +96,11 @@ int pff_accumulate(const int32_t *receivers, float *Q, uint32_t *counts, int N, 
 int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t *counts, int nx, int ny,
                         int bound_mode, const uint8_t *codes, int N, void *workspace,
                         size_t workspace_bytes, void *stream);
+/* Tuning switch of pff_accumulate_grid (no reference counterpart): the number of
+ * leading rounds (3 default, 4, or 0 = off) run per spatial tile in shared memory
+ * for boundary modes 0-2 on grids of at least 3 x 3.  Every setting gives the same
+ * results.  Process-wide; returns PFF_ERR_ARG for other values. */
+int pff_accumulate_set_front(int rounds);
 
 /* ---- lake / depression rerouting -----------------------------------------------
  * Replaces pyfastflow/flow/lakeflow.py:466-538 reroute_flow(bid, rec, rec_, rec__,

@@ -446,55 +446,6 @@ __global__ void k_basin_reset_list(long long *saddle, long long *outlet, int32_t
     }
 }
 
-// pass 1+2 as k_saddle_p12, also listing the border cells for pass 3
-template <int MODE>
-__global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restrict__ bid, uint8_t *is_border,
-                                                         float *zp, long long *saddle, const float *__restrict__ z,
-                                                         Grid g, int *blist, int *nblist)
-{
-    const int col = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int row = blockIdx.y * 8 + (threadIdx.x >> 5);
-    const bool in = col < g.nx && row < g.ny;
-    const int i = row * g.nx + col;
-    bool border = false;
-    if (in) {
-        const float zi = z[i];
-        if (can_leave<MODE>(g, i, row, col)) {
-            zp[i] = zi;
-        } else {
-            const int bi = bid[i];
-            int js[4];
-            neighbours4<MODE>(g, i, row, col, js);
-            float zn = 1e9f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int j = js[k];
-                if (j != -1 && bid[j] != bi) { border = true; zn = fminf(zn, z[j]); }
-            }
-            is_border[i] = border;
-            const float zpi = border ? fmaxf(zi, zn) : 1e9f;
-            zp[i] = zpi;
-            if (border) {
-                const long long iv = invalid_key();
-                long long res = iv;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int j = js[k];
-                    if (j == -1) continue;
-                    const int bj = bid[j];
-                    if (bj != bi) {
-                        const long long c = pack_key(zpi, bj);
-                        res = c < res ? c : res;
-                    }
-                }
-                if (res != iv) atomicMin(saddle + bi, res);
-            }
-        }
-    }
-    // one atomic per block: a per-warp atomic on this single counter serialises in L2
-    block_append<256>(border && bid[i] != 0, i, blist, nblist);
-}
-
 // Pass 1+2 as a column-strip stencil: each warp walks a 32-column strip down
 // SAD_ROWS rows with bid and z of the rows above/at/below in registers and the
 // left/right values from neighbouring lanes.  Border cells of pit basins collect
@@ -502,10 +453,12 @@ __global__ void __launch_bounds__(256) k_saddle_p12_list(const int32_t *__restri
 constexpr int SAD_ROWS = 32;
 constexpr int SAD_AHEAD = 4;  // rows loaded per group (SAD_ROWS is a multiple)
 
+// Returns 0 for a cell off every border, 1 for a border cell of the outlet
+// basin 0, 2 for a border cell of a pit basin.
 template <int MODE>
-__device__ __forceinline__ bool saddle_cell(int i, int row, int col, const Grid &g, int bi, float zi, const int (&jn)[4],
-                                            const int (&bn)[4], const float (&zn)[4], uint8_t *is_border, float *zp,
-                                            long long *saddle)
+__device__ __forceinline__ int saddle_cell(int i, int row, int col, const Grid &g, int bi, float zi, const int (&jn)[4],
+                                           const int (&bn)[4], const float (&zn)[4], uint8_t *is_border, float *zp,
+                                           long long *saddle)
 {
     bool border = false;
     float zmin = 1e9f;
@@ -515,7 +468,7 @@ __device__ __forceinline__ bool saddle_cell(int i, int row, int col, const Grid 
     is_border[i] = border;
     const float zpi = border ? fmaxf(zi, zmin) : 1e9f;
     zp[i] = zpi;
-    if (!border) return false;
+    if (!border) return 0;
     const long long iv = invalid_key();
     long long res = iv;
 #pragma unroll
@@ -525,13 +478,13 @@ __device__ __forceinline__ bool saddle_cell(int i, int row, int col, const Grid 
         res = c < res ? c : res;
     }
     if (res != iv) atomicMin(saddle + bi, res);
-    return bi != 0;
+    return bi != 0 ? 2 : 1;
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restrict__ bid, uint8_t *is_border,
                                                           float *zp, long long *saddle, const float *__restrict__ z,
-                                                          Grid g, int *blist, int *nblist)
+                                                          Grid g, int *blist, int *nblist, int *alist, int *nalist)
 {
     __shared__ int buf[4][32 * SAD_ROWS];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -578,7 +531,7 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
             const float zb = zq[q];
             int bl = __shfl_up_sync(0xffffffffu, bc, 1), br = __shfl_down_sync(0xffffffffu, bc, 1);
             float zl = __shfl_up_sync(0xffffffffu, zc, 1), zr = __shfl_down_sync(0xffffffffu, zc, 1);
-            bool listed = false;
+            int listed = 0;  // saddle_cell's code
             if (incol) {
                 const bool interior = MODE != 3 && rw > 0 && rw < ny - 1 && col > 0 && col < nx - 1;
                 if (interior) {
@@ -603,18 +556,72 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
                     listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
                 }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, listed);
-            if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = i;
+            // every border cell, the pit-basin ones marked by the sign bit
+            const unsigned m = __ballot_sync(0xffffffffu, listed != 0);
+            if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = listed == 2 ? (i | (int)0x80000000) : i;
             nb += __popc(m);
             ba = bc; bc = bb;
             za = zc; zc = zb;
         }
     }
     __syncwarp();
-    int base = 0;
-    if (lane == 0 && nb) base = atomicAdd(nblist, nb);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    for (int k = lane; k < nb; k += 32) blist[base + k] = buf[wib][k];
+    int npit = 0;
+    for (int k = lane; k < nb; k += 32) npit += buf[wib][k] < 0;
+    npit = __reduce_add_sync(0xffffffffu, npit);
+    int bp = 0, bq = 0;  // bases in blist and alist
+    if (lane == 0) {
+        if (npit) bp = atomicAdd(nblist, npit);
+        if (alist && nb) bq = atomicAdd(nalist, nb);
+    }
+    bp = __shfl_sync(0xffffffffu, bp, 0);
+    bq = __shfl_sync(0xffffffffu, bq, 0);
+    int run = 0;
+    for (int k0 = 0; k0 < nb; k0 += 32) {
+        const int k = k0 + lane;
+        const int v = k < nb ? buf[wib][k] : 0;
+        const bool pit = k < nb && v < 0;
+        const int i = v & 0x7FFFFFFF;
+        if (alist && k < nb) alist[bq + k] = i;
+        const unsigned m = __ballot_sync(0xffffffffu, pit);
+        if (pit) blist[bp + run + __popc(m & ((1u << lane) - 1u))] = i;
+        run += __popc(m);
+    }
+}
+
+// Pass 1+2 of a later outer iteration over the border cells of the previous one.
+// Labels change between outer iterations only by merging basins (b -> fin(b)), so
+// a cell whose neighbours all shared its label still does, keeps is_border = 0
+// and z' = 1e9, and contributes no saddle: only the previous border cells can
+// change.  Lists the cells still on a border (all, and those of pit basins).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_saddle_p12_border(const int32_t *__restrict__ bid, uint8_t *is_border,
+                                                           float *zp, long long *saddle, const float *__restrict__ z,
+                                                           Grid g, const int *__restrict__ aprev, const int *naprev,
+                                                           int *anext, int *nanext, int *blist, int *nblist)
+{
+    const int n = *naprev;
+    const int stride = gridDim.x * 256;
+    const int trips = (n + stride - 1) / stride;
+    for (int k = 0; k < trips; ++k) {
+        const int idx = k * stride + blockIdx.x * 256 + threadIdx.x;
+        int code = 0, i = -1;
+        if (idx < n) {
+            i = aprev[idx];
+            const int row = i / g.nx, col = i - row * g.nx;
+            int jn[4], bn[4];
+            float zn[4];
+            neighbours4<MODE>(g, i, row, col, jn);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                bn[q] = jn[q] != -1 ? bid[jn[q]] : 0;
+                zn[q] = jn[q] != -1 ? z[jn[q]] : 0.f;
+            }
+            // an outlet is never listed (its z' is z and it has no border status)
+            code = saddle_cell<MODE>(i, row, col, g, bid[i], z[i], jn, bn, zn, is_border, zp, saddle);
+        }
+        block_append<256>(code != 0, i, anext, nanext);
+        block_append<256>(code == 2, i, blist, nblist);
+    }
 }
 
 template <int MODE>
@@ -1082,11 +1089,18 @@ static void l_cycle_emulate(const int32_t *rec, const int *entries, const int *n
 template <int MODE>
 static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long long *saddle, int32_t *snode,
                            long long *outlet, uint8_t *inv, const float *z, const Grid &g, const int *pits,
-                           const int *np, int *blist, int *nblist, int grid, cudaStream_t st)
+                           const int *np, int *blist, int *nblist, const int *aprev, const int *naprev, int *anext,
+                           int *nanext, int grid, cudaStream_t st)
 {
     const int N = g.N();
-    const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + SAD_ROWS - 1) / SAD_ROWS);
-    { k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist); count_launch(); }
+    if (!aprev) {
+        const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + SAD_ROWS - 1) / SAD_ROWS);
+        { k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist, anext,
+                                                                     nanext); count_launch(); }
+    } else {
+        { k_saddle_p12_border<MODE><<<grid, 256, 0, st>>>(bid, isb, zp, saddle, z, g, aprev, naprev, anext, nanext,
+                                                           blist, nblist); count_launch(); }
+    }
     { k_saddle_p3_list<MODE><<<grid, 256, 0, st>>>(bid, zp, saddle, snode, g, blist, nblist); count_launch(); }
     { k_saddle_p4_list<MODE><<<grid, 256, 0, st>>>(bid, saddle, snode, outlet, z, g, pits, np); count_launch(); }
     { k_saddle_p5_decide_list<<<grid, 256, 0, st>>>(bid, outlet, inv, N, pits, np); count_launch(); }
@@ -1185,7 +1199,7 @@ extern "C" int pff_saddlesort(const int32_t *bid, uint8_t *is_border, float *z_p
 extern "C" size_t pff_reroute_workspace_bytes(int N)
 {
     const size_t n = (size_t)N;
-    return Carver::round(n + 1) * 2 + Carver::round(4 * (n + 1)) + Carver::round(4 * n) * 6 + Carver::round(8 * n) +
+    return Carver::round(n + 1) * 2 + Carver::round(4 * (n + 1)) + Carver::round(4 * n) * 8 + Carver::round(8 * n) +
            Carver::round(sizeof(int) * 512) + 8192;
 }
 
@@ -1198,8 +1212,10 @@ struct RerouteWs {
     int *tiles;
     int *pits[2];
     int *blist, *segs;
+    int *alist[2];  // every border cell of a saddlesort (parity of the outer iteration)
     int *ctr;  // [16*p + 0] pits, +2 non-D4 flag (parity p); [40] nblist, [41] nsegs, [42] nmods,
-               // [43] error; [44] dirty tiles; [45] odd carve; [64..127] border-jump round flags;
+               // [43] error; [44] dirty tiles; [45] odd carve; [50 + p] alist[p] count;
+               // [64..127] border-jump round flags;
                // [128..191] label round flags; [192..255] carve round flags; [256..319] relabel flags
 };
 
@@ -1216,6 +1232,8 @@ static RerouteWs carve_ws(void *workspace, size_t bytes, int N)
     w.pits[1] = cv.take<int>(N);
     w.blist = cv.take<int>(N);
     w.segs = cv.take<int>(N);
+    w.alist[0] = cv.take<int>(N);
+    w.alist[1] = cv.take<int>(N);
     w.ctr = cv.take<int>(512);
     return w;
 }
@@ -1379,8 +1397,12 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
                                                          w.ctr + 16 * (par ^ 1)); count_launch(); }
             }
             PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 6 * sizeof(int), st));
+            PFF_CUDA(cudaMemsetAsync(w.ctr + 50 + par, 0, sizeof(int), st));
+            // it > 0 here means every earlier iteration took this path: labels only merged since
+            const int *aprev = it == 0 ? nullptr : w.alist[par ^ 1];
             PFF_MODE_DISPATCH(bound_mode, l_saddle_lists, bid, is_border, z_prime, sad, basin_saddlenode, out, w.inv, z,
-                              g, w.pits[par], np, w.blist, w.ctr + 40, grid, st);
+                              g, w.pits[par], np, w.blist, w.ctr + 40, aprev, w.ctr + 50 + (par ^ 1), w.alist[par],
+                              w.ctr + 50 + par, grid, st);
         }
         if (!carve) {
             { k_carve_link_outlets<<<nbk, B, 0, st>>>(rec_, basin_saddlenode, out, N, 1); count_launch(); }  // :529

@@ -744,39 +744,127 @@ __device__ __forceinline__ int walk_segment(int start, const int32_t *__restrict
     return -1;
 }
 
-// Per basin with a saddle node: walk the first segment (in the saddle node's
-// tile) directly, then hop tile by tile through J and list the later segment
-// starts for k_carve_walk.
-__global__ void k_carve_segments(const int32_t *__restrict__ snode, const int32_t *__restrict__ rec0, int32_t *rec,
-                                 uint8_t *tag, uint8_t *tag_, const int32_t *__restrict__ J,
-                                 const int *__restrict__ pits, const int *np, int N, int nx, int *segs, int *nsegs,
-                                 int cap, int *err, uint8_t *dirty)
+// Per basin with a saddle node: list the saddle node and every later segment
+// start, hopping tile by tile through J (J[x] is the first cell past x's tile on
+// its path, or its root).  Each warp takes 32 basins and hops them in lockstep;
+// the starts collect in a per-warp shared buffer that goes out with one atomic
+// when nearly full.  The paths are disjoint, so N slots suffice.
+constexpr int SEG_WARPS = 4, SEG_CAP = 512;
+
+__global__ void __launch_bounds__(32 * SEG_WARPS) k_carve_segments(const int32_t *__restrict__ snode,
+                                                                   const int32_t *__restrict__ rec0,
+                                                                   const int32_t *__restrict__ J,
+                                                                   const int *__restrict__ pits, const int *np, int N,
+                                                                   int *segs, int *nsegs, int cap, int *err)
 {
+    __shared__ int buf[SEG_WARPS][SEG_CAP];
     const int n = *np;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int b = pits[k] + 1;
-        if (b >= N) continue;
-        const int s0 = snode[b];
-        if (s0 < 0) continue;
-        int x = walk_segment(s0, rec0, rec, tag, tag_, nx, dirty);
-        // x is now the first cell outside the saddle node's tile (or -1 at the pit);
-        // J hops from there give every later segment start
-        for (int step = 0; x >= 0 && step < N; ++step) {
-            const int slot = atomicAdd(nsegs, 1);
-            if (slot < cap) segs[slot] = x;
-            else { *err = 1; break; }
-            if (rec0[x] == x) break;
-            x = J[x];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int nb = 0;  // warp-uniform
+    auto flush = [&]() {
+        __syncwarp();
+        int base = 0;
+        if (lane == 0 && nb) base = atomicAdd(nsegs, nb);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        for (int q = lane; q < nb; q += 32) {
+            if (base + q < cap) segs[base + q] = buf[wib][q];
+            else *err = 1;
+        }
+        __syncwarp();
+        nb = 0;
+    };
+    for (int kb = (blockIdx.x * SEG_WARPS + wib) * 32; kb < n; kb += gridDim.x * SEG_WARPS * 32) {
+        const int k = kb + lane;
+        int x = -1;
+        if (k < n) {
+            const int b = pits[k] + 1;
+            if (b < N) x = snode[b];
+        }
+        for (int step = 0; step <= N && __any_sync(0xffffffffu, x >= 0); ++step) {
+            const bool emit = x >= 0;
+            const unsigned m = __ballot_sync(0xffffffffu, emit);
+            if (emit) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = x;
+            nb += __popc(m);
+            if (nb > SEG_CAP - 32) flush();
+            if (emit) x = rec0[x] == x ? -1 : J[x];
         }
     }
+    flush();
 }
 
-__global__ void k_carve_walk(const int32_t *__restrict__ rec0, int32_t *rec, uint8_t *tag, uint8_t *tag_,
-                             const int *__restrict__ segs, const int *nsegs, int cap, int nx, uint8_t *dirty)
+// Walk the listed segments.  With more than WALK_BLOCK_MAX segments, one thread
+// walks each in global memory (walk_segment).  Otherwise one block takes a segment:
+// it loads the segment's tile with every receiver as a tile-local index (or
+// ~target when the receiver lies past the tile), tags the segment's cells by
+// pointer doubling (after round r every cell within 2^(r+1) - 1 steps of the
+// start is tagged), then makes walk_segment's writes for the tagged cells in
+// parallel: tag, tag_, rec[receiver] = cell, and the dirty tiles.
+constexpr int WALK_THREADS = 256, WALK_BLOCK_MAX = 4096;
+
+__global__ void __launch_bounds__(WALK_THREADS) k_carve_walk(const int32_t *__restrict__ rec0, int32_t *rec,
+                                                             uint8_t *tag, uint8_t *tag_,
+                                                             const int *__restrict__ segs, const int *nsegs, int cap,
+                                                             int nx, int ny, uint8_t *dirty)
 {
+    __shared__ int nl[TILE_CELLS];
+    __shared__ int16_t jmp[2][TILE_CELLS];
+    __shared__ uint8_t on[TILE_CELLS];
     const int n = min(*nsegs, cap);
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        walk_segment(segs[k], rec0, rec, tag, tag_, nx, dirty);
+    if (n > WALK_BLOCK_MAX) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+            walk_segment(segs[k], rec0, rec, tag, tag_, nx, dirty);
+        return;
+    }
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s0 = segs[k];
+    static_assert(TILE_W == 64, "local index = row * 64 + column");
+    const int srow = s0 / nx, scol = s0 - srow * nx;
+    const int ty = srow / TILE_H, tx = scol / TILE_W;
+    const int r0 = ty * TILE_H, c0 = tx * TILE_W;
+    const int h = min(TILE_H, ny - r0), w = min(TILE_W, nx - c0);
+    const int start = ((srow - r0) << 6) | (scol - c0);
+    for (int q = threadIdx.x; q < TILE_CELLS; q += WALK_THREADS) {
+        const int lr = q >> 6, lc = q & 63;
+        int v = q;  // cells past the grid edge: terminal, never reached
+        if (lr < h && lc < w) {
+            const int r = rec0[(r0 + lr) * nx + c0 + lc];
+            const int rr = r / nx, rc = r - rr * nx;
+            v = (rr / TILE_H == ty && rc / TILE_W == tx) ? (((rr - r0) << 6) | (rc - c0)) : ~r;
+        }
+        nl[q] = v;
+        jmp[0][q] = (int16_t)((v >= 0 && v != q) ? v : -1);
+        on[q] = q == start;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int r = 0; r < 11; ++r) {  // 2^11 = TILE_CELLS
+        const int16_t *jc = jmp[r & 1];
+        int16_t *jn = jmp[(r & 1) ^ 1];
+        for (int q = threadIdx.x; q < TILE_CELLS; q += WALK_THREADS) {
+            const int j = jc[q];
+            if (on[q] && j >= 0) on[j] = 1;
+            jn[q] = j >= 0 ? jc[j] : (int16_t)-1;
+        }
+        __syncthreads();
+    }
+    bool local_write = false;
+    for (int q = threadIdx.x; q < TILE_CELLS; q += WALK_THREADS) {
+        if (!on[q]) continue;
+        const int gq = (r0 + (q >> 6)) * nx + c0 + (q & 63);
+        tag[gq] = 1;
+        tag_[gq] = 1;
+        const int v = nl[q];
+        if (v == q) continue;  // the root
+        if (v < 0) {
+            rec[~v] = gq;  // the path leaves the tile
+            mark_tile(dirty, nx, ~v);
+        } else {
+            rec[(r0 + (v >> 6)) * nx + c0 + (v & 63)] = gq;
+            local_write = true;
+        }
+    }
+    if (__syncthreads_or(local_write) && threadIdx.x == 0) mark_tile(dirty, nx, s0);
+    }
 }
 
 __global__ void k_carve_link_list(int32_t *rec, const int32_t *__restrict__ snode, const long long *__restrict__ outlet,
@@ -1436,9 +1524,10 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
             continue;
         }
         // rec == rec_ here; rec__ holds the tile terminals of rec_
-        { k_carve_segments<<<grid, B, 0, st>>>(basin_saddlenode, rec_, rec, tag, tag_, rec__, w.pits[par], np, N, nx,
-                                               w.segs, w.ctr + 41, N, w.ctr + 43, w.dirty); count_launch(); }
-        { k_carve_walk<<<grid, B, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, w.dirty); count_launch(); }
+        { k_carve_segments<<<nsm * 4, 32 * SEG_WARPS, 0, st>>>(basin_saddlenode, rec_, rec__, w.pits[par], np, N,
+                                                                 w.segs, w.ctr + 41, N, w.ctr + 43); count_launch(); }
+        { k_carve_walk<<<nsm * 4, WALK_THREADS, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, g.ny,
+                                                          w.dirty); count_launch(); }
         { k_carve_link_list<<<grid, B, 0, st>>>(rec, basin_saddlenode, out, w.pits[par], np, N, w.dirty, nx); count_launch(); }
         { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0); count_launch(); }  // :526
         // ---- next iteration: pits left, labels by basin relabelling, dirty tiles ----

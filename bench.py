@@ -78,6 +78,7 @@ class Clocks:
         self.proc = None
         self.stop = threading.Event()
         self.t = None
+        self.error = None
 
     def _nvml_handle(self):
         import pynvml
@@ -91,12 +92,15 @@ class Clocks:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
 
     def _poll(self, nv, h):
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while not self.stop.is_set():
-            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
-            self.rows.append((float(sm), float(mx), [k for k, b in self.REASONS.items() if bits & b]))
-            self.stop.wait(0.005)
+        try:
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self.stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((float(sm), float(mx), [k for k, b in self.REASONS.items() if bits & b]))
+                self.stop.wait(0.005)
+        except Exception as e:  # reported in the summary
+            self.error = f"{type(e).__name__}: {e}"
 
     def __enter__(self):
         try:
@@ -104,8 +108,8 @@ class Clocks:
             self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
             self.t.start()
             return self
-        except Exception:
-            pass
+        except Exception as e:
+            self.error = f"{type(e).__name__}: {e}"
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -136,7 +140,10 @@ class Clocks:
 
     def summary(self):
         if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            if self.error:
+                out["error"] = self.error
+            return out
         return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
                 "reasons": sorted({x for r in self.rows for x in r[2]}), "samples": len(self.rows),
                 "source": "nvml" if self.proc is None else "nvidia-smi"}

@@ -1536,19 +1536,9 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         { k_relabel_init<<<grid, B, 0, st>>>(w.fin, bid, basin_saddlenode, out, w.pits[par], np, N, w.pits[par ^ 1],
                                              np_next, w.ctr + 45); count_launch(); }
         { k_dirty_list<<<div_up(ntiles, B), B, 0, st>>>(w.dirty, ntiles, w.tiles, w.ctr + 44); count_launch(); }
-        int h[3];
-        PFF_CUDA(cudaMemcpyAsync(h, w.ctr + 43, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaMemcpyAsync(&nd_next, np_next, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaStreamSynchronize(st));
-        if (h[0]) break;  // walk bounds exceeded: reported below
-        const int ndirty = h[1];
-        if (h[2]) {
-            // a reversed path without an outlet link (elevations >= 1e9 only)
-            general = true;
-            continue;
-        }
-        if (it + 1 >= outer) break;  // :500
-        // the basin relabelling; a basin chain that does not converge is a cycle
+        // The basin relabelling, launched before the host reads this iteration's
+        // flags so that one synchronisation serves both; its result is used only
+        // if the loop goes on.  A basin chain that does not converge is a cycle.
         int *flags = w.ctr + 256;
         PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), st));
         static int coop_relabel = 0;
@@ -1564,9 +1554,19 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         int *cyc = w.ctr + 49;
         PFF_CUDA(cudaMemsetAsync(cyc, 0, sizeof(int), st));
         { k_relabel_check<<<grid, B, 0, st>>>(w.fin, out, w.pits[par], np, N, cyc); count_launch(); }
-        int hc = 0;
+        int h[3], hc = 0;
+        PFF_CUDA(cudaMemcpyAsync(h, w.ctr + 43, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        PFF_CUDA(cudaMemcpyAsync(&nd_next, np_next, sizeof(int), cudaMemcpyDeviceToHost, st));
         PFF_CUDA(cudaMemcpyAsync(&hc, cyc, sizeof(int), cudaMemcpyDeviceToHost, st));
         PFF_CUDA(cudaStreamSynchronize(st));
+        if (h[0]) break;  // walk bounds exceeded: reported below
+        const int ndirty = h[1];
+        if (h[2]) {
+            // a reversed path without an outlet link (elevations >= 1e9 only)
+            general = true;
+            continue;
+        }
+        if (it + 1 >= outer) break;  // :500
         if (trace) fprintf(stderr, "[pff reroute]   after carve: next pits %d dirty %d cycle %d\n", nd_next, ndirty, hc);
         if (hc) {
             general = true;  // the carve closed a receiver cycle: the reference's path from here on

@@ -944,22 +944,32 @@ __global__ void __launch_bounds__(256) k_relabel_jump_coop(int32_t *fin, const i
     }
 }
 
-// four cells per thread; label 0 (outlet basins) never changes
-__global__ void __launch_bounds__(256) k_relabel(int32_t *bid, const int32_t *__restrict__ fin, int N, int vec)
+// four cells per thread; label 0 (outlet basins) never changes.  The same pass
+// makes rec_ = rec on the carved cells (k_sync_tagged's copy, :526).
+__global__ void __launch_bounds__(256) k_relabel(int32_t *bid, const int32_t *__restrict__ fin, int32_t *rec_,
+                                                 const int32_t *__restrict__ rec, const uint8_t *__restrict__ tag,
+                                                 int N, int vec)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = 4 * q;
     if (vec && i + 3 < N) {
         int4 b = reinterpret_cast<int4 *>(bid)[q];
+        const uchar4 t = reinterpret_cast<const uchar4 *>(tag)[q];
         const int4 o = b;
         if (b.x) b.x = fin[b.x];
         if (b.y) b.y = fin[b.y];
         if (b.z) b.z = fin[b.z];
         if (b.w) b.w = fin[b.w];
         if (b.x != o.x || b.y != o.y || b.z != o.z || b.w != o.w) reinterpret_cast<int4 *>(bid)[q] = b;
+        if (t.x) rec_[i] = rec[i];
+        if (t.y) rec_[i + 1] = rec[i + 1];
+        if (t.z) rec_[i + 2] = rec[i + 2];
+        if (t.w) rec_[i + 3] = rec[i + 3];
     } else {
-        for (int k = i; k < N && k < i + 4; ++k)
+        for (int k = i; k < N && k < i + 4; ++k) {
             if (bid[k]) bid[k] = fin[bid[k]];
+            if (tag[k]) rec_[k] = rec[k];
+        }
     }
 }
 
@@ -1529,7 +1539,6 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         { k_carve_walk<<<nsm * 4, WALK_THREADS, 0, st>>>(rec_, rec, tag, tag_, w.segs, w.ctr + 41, N, nx, g.ny,
                                                           w.dirty); count_launch(); }
         { k_carve_link_list<<<grid, B, 0, st>>>(rec, basin_saddlenode, out, w.pits[par], np, N, w.dirty, nx); count_launch(); }
-        { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0); count_launch(); }  // :526
         // ---- next iteration: pits left, labels by basin relabelling, dirty tiles ----
         int *np_next = w.ctr + 16 * (par ^ 1);
         PFF_CUDA(cudaMemsetAsync(np_next, 0, 4 * sizeof(int), st));
@@ -1559,6 +1568,11 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         PFF_CUDA(cudaMemcpyAsync(&nd_next, np_next, sizeof(int), cudaMemcpyDeviceToHost, st));
         PFF_CUDA(cudaMemcpyAsync(&hc, cyc, sizeof(int), cudaMemcpyDeviceToHost, st));
         PFF_CUDA(cudaStreamSynchronize(st));
+        // rec_ = rec on the carved cells (:526): inside the relabelling pass when
+        // the loop goes on, else here
+        if (h[0] || h[2] || it + 1 >= outer || hc || nd_next == 0) {
+            { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0); count_launch(); }
+        }
         if (h[0]) break;  // walk bounds exceeded: reported below
         const int ndirty = h[1];
         if (h[2]) {
@@ -1576,7 +1590,8 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
             ++n_outer;  // the next iteration would count 0 pits, label, then break (:512-514)
             break;      // its labels are reset by basin_id_init (:537) anyway
         }
-        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, N, ((uintptr_t)bid & 15) == 0); count_launch(); }
+        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, rec_, rec, tag, N,
+                                                           ((uintptr_t)bid & 15) == 0 && ((uintptr_t)tag & 3) == 0); count_launch(); }
         PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, ndirty, st);
         incremental = true;
         PFF_TRY(check_cuda("pff_reroute_flow"));

@@ -938,8 +938,7 @@ extern "C" int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t 
     }
     PFF_TRY(check_cuda("pff_accumulate"));
     int over = 0;
-    PFF_CUDA(cudaMemcpyAsync(&over, overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PFF_CUDA(cudaStreamSynchronize(st));
+    PFF_TRY(read_ints(IntReads().add(overflow, 1), &over, st));
     if (over) {
         set_error("pff_accumulate: a node has more than 4 donors (possible only after jump rerouting); "
                   "the reference's donor slots overflow there and this case is not supported");

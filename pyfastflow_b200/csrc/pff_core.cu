@@ -393,6 +393,50 @@ extern "C" int pff_compute_receivers_stochastic(const float *z, int32_t *receive
 
 extern "C" int pff_version(void) { return 100; }
 extern "C" const char *pff_last_error_string(void) { return g_err; }
+namespace pff {
+
+__global__ void k_read_ints(IntReads r, volatile int *dst)
+{
+    int o = 0;
+    for (int a = 0; a < r.k; ++a)
+        for (int q = 0; q < r.n[a]; ++q) dst[o++] = r.src[a][q];
+    __threadfence_system();
+}
+
+// One mapped pinned buffer per host thread and device (256 bytes each, kept
+// until the process exits).
+int read_ints(const IntReads &r, int *out, cudaStream_t st)
+{
+    static thread_local int *host_buf[64] = {nullptr};
+    int dev = 0;
+    PFF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || r.k > 8) {
+        set_error("read_ints: device %d or %d reads out of range", dev, r.k);
+        return PFF_ERR_ARG;
+    }
+    int total = 0;
+    for (int a = 0; a < r.k; ++a) total += r.n[a];
+    if (total > 64) {
+        set_error("read_ints: %d ints exceed 64", total);
+        return PFF_ERR_ARG;
+    }
+    if (!host_buf[dev]) {
+        void *p = nullptr;
+        PFF_CUDA(cudaHostAlloc(&p, 64 * sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+        host_buf[dev] = (int *)p;
+    }
+    int *dptr = nullptr;
+    PFF_CUDA(cudaHostGetDevicePointer((void **)&dptr, host_buf[dev], 0));
+    { k_read_ints<<<1, 1, 0, st>>>(r, dptr); count_launch(); }
+    PFF_CUDA(cudaStreamSynchronize(st));
+    PFF_TRY(check_cuda("read_ints"));
+    const volatile int *h = host_buf[dev];
+    for (int q = 0; q < total; ++q) out[q] = h[q];
+    return PFF_OK;
+}
+
+}  // namespace pff
+
 extern "C" long long pff_launch_count(void) { return g_launches.load(); }
 
 extern "C" int pff_set_device(int device)

@@ -37,6 +37,24 @@ int check_cuda(const char *where);
 
 int check_grid(int nx, int ny, int mode, const uint8_t *codes);
 
+// Read small device int arrays (a list of (pointer, count), at most 8 pointers and
+// 64 ints) into host memory, in order, and synchronise `st`.  A one-thread kernel
+// stores them into mapped pinned host memory, so the read uses no copy engine and
+// does not wait behind bulk transfers other streams have in flight.
+struct IntReads {
+    const int *src[8];
+    int n[8];
+    int k = 0;
+    IntReads &add(const int *p, int cnt)
+    {
+        src[k] = p;
+        n[k++] = cnt;
+        return *this;
+    }
+};
+int read_ints(const IntReads &r, int *out, cudaStream_t st);
+
+
 // Bump allocator over a caller-provided device workspace (256-byte aligned slices).
 struct Carver {
     char *base;

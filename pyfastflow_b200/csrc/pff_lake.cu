@@ -1235,10 +1235,7 @@ int count_pits(const int32_t *rec, const Grid &g, int *dev_count, int *pit_list,
     PFF_CUDA(cudaMemsetAsync(dev_count, 0, sizeof(int), st));
     PFF_MODE_DISPATCH(g.mode, l_count_pits, rec, g, dev_count, pit_list, st);
     PFF_TRY(check_cuda("depression_counter"));
-    if (host_count) {
-        PFF_CUDA(cudaMemcpyAsync(host_count, dev_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaStreamSynchronize(st));
-    }
+    if (host_count) PFF_TRY(read_ints(IntReads().add(dev_count, 1), host_count, st));
     return PFF_OK;
 }
 
@@ -1346,8 +1343,7 @@ static int tile_pass(const int32_t *rec, int32_t *Jbuf, const Grid &g, RerouteWs
     PFF_CUDA(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
     PFF_MODE_DISPATCH(g.mode, l_tile_terminal, rec, Jbuf, w.R, w.pits[parity], info, g, st);
     int h[4];
-    PFF_CUDA(cudaMemcpyAsync(h, info, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    PFF_CUDA(cudaStreamSynchronize(st));
+    PFF_TRY(read_ints(IntReads().add(info, 4), h, st));
     *npits_host = h[0];
     *nonlocal_host = h[2];
     return check_cuda("tile_pass");
@@ -1460,8 +1456,7 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         } else {
             PFF_CUDA(cudaMemsetAsync(np, 0, 4 * sizeof(int), st));
             PFF_MODE_DISPATCH(g.mode, l_count_pits, rec_, g, np, w.pits[par], st);  // :501
-            PFF_CUDA(cudaMemcpyAsync(&nd_bis, np, sizeof(int), cudaMemcpyDeviceToHost, st));
-            PFF_CUDA(cudaStreamSynchronize(st));
+            PFF_TRY(read_ints(IntReads().add(np, 1), &nd_bis, st));
         }
         if (it == 0) {
             if (nd_bis == 0) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
@@ -1473,8 +1468,7 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
             PFF_CUDA(cudaMemsetAsync(unres, 0, sizeof(int), st));
             PFF_TRY(tile_resolve(rec__, bid, g, w, rec_, unres, st));
             int u = 0;
-            PFF_CUDA(cudaMemcpyAsync(&u, unres, sizeof(int), cudaMemcpyDeviceToHost, st));
-            PFF_CUDA(cudaStreamSynchronize(st));
+            PFF_TRY(read_ints(IntReads().add(unres, 1), &u, st));
             if (u) general = true;  // the input receivers hold a cycle
         }
         if (general) PFF_TRY(general_labels(rec_, rec__, bid, g, w, cyc_err, st));
@@ -1563,11 +1557,10 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         int *cyc = w.ctr + 49;
         PFF_CUDA(cudaMemsetAsync(cyc, 0, sizeof(int), st));
         { k_relabel_check<<<grid, B, 0, st>>>(w.fin, out, w.pits[par], np, N, cyc); count_launch(); }
-        int h[3], hc = 0;
-        PFF_CUDA(cudaMemcpyAsync(h, w.ctr + 43, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaMemcpyAsync(&nd_next, np_next, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaMemcpyAsync(&hc, cyc, sizeof(int), cudaMemcpyDeviceToHost, st));
-        PFF_CUDA(cudaStreamSynchronize(st));
+        int hv[5];
+        PFF_TRY(read_ints(IntReads().add(w.ctr + 43, 3).add(np_next, 1).add(cyc, 1), hv, st));
+        const int h[3] = {hv[0], hv[1], hv[2]}, hc = hv[4];
+        nd_next = hv[3];
         // rec_ = rec on the carved cells (:526): inside the relabelling pass when
         // the loop goes on, else here
         if (h[0] || h[2] || it + 1 >= outer || hc || nd_next == 0) {
@@ -1597,9 +1590,8 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         PFF_TRY(check_cuda("pff_reroute_flow"));
     }
     int err[5] = {0, 0, 0, 0, 0};
-    PFF_CUDA(cudaMemcpyAsync(err, w.ctr + 43, 5 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PFF_TRY(launch_basin_init(bid, g, st));  // :537
-    PFF_CUDA(cudaStreamSynchronize(st));
+    PFF_TRY(read_ints(IntReads().add(w.ctr + 43, 5), err, st));
     if (err[0]) {
         set_error("pff_reroute_flow: carve walk exceeded its bounds");
         return PFF_ERR_NOCONV;

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(BS, 5) k_acc_round(const Pub *__restrict__ cur
             }
             // Every donor state this round can need is one of the start-of-round
             // slots: load them all up front (independent loads).  The reference's
-            // swap-remove scan (downstream_propag.py:187-220) then runs on
+            // swap-remove scan (downstream_propag.py:131-162) then runs on
             // registers: slot k holds donor w_k whose preloaded state is q_k.
             Pub P0 = s, P1 = s, P2 = s, P3 = s;
             if (todo > 0) P0 = cur[own[0]];

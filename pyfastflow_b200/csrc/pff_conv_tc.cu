@@ -17,8 +17,10 @@
 // one issues MMAs and commits each stage back to the producer; after the last
 // commit the 4 warps read the 128 x N accumulator with tcgen05.ld (warp w owns
 // TMEM lanes 32w..32w+31 = pixels), add the bias, apply ReLU and store bf16 or f32.
-// Every mbarrier wait is bounded; a wait that runs out sets an error flag, and the
-// kernel still frees its TMEM and returns.
+// Every mbarrier wait is bounded; a wait that runs out sets an error flag.  The
+// block then waits (again bounded) for every TMA load it issued but did not
+// consume, so that no bulk copy is still writing its shared memory when it frees
+// its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include "pff_internal.h"
@@ -138,6 +140,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3x3_tc(const __grid_constant
     __shared__ __align__(8) uint64_t full[TC_ST], empty[TC_ST], done;
     __shared__ unsigned tmem_base;
     __shared__ int failed;
+    __shared__ int issued, consumed;  // TMA stages issued by the producer / waited for by the MMA issuer
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     const int tiles_x = a.W / a.BW, tiles_y = a.H / a.BH;
@@ -158,6 +161,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3x3_tc(const __grid_constant
         }
         mbar_init(&done, 1);
         failed = 0;
+        issued = 0;
+        consumed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 0) {  // TMEM: BN f32 columns x 128 lanes
@@ -171,21 +176,27 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3x3_tc(const __grid_constant
     const unsigned tmem = tmem_base;
 
     if (warp == 0 && lane == 0) {  // producer
+        int n = 0;
         for (int it = 0; it < nk; ++it) {
             const int s = it % TC_ST;
             if (it >= TC_ST && !mbar_wait(&empty[s], ((it / TC_ST) - 1) & 1)) { failed = 1; break; }
+            if (*(volatile int *)&failed) break;  // the MMA issuer gave up: issue nothing more
             const int tap = it / kchunks, kc = it - tap * kchunks;
             const int dy = tap / 3 - 1, dx = tap % 3 - 1;
             mbar_expect_tx(&full[s], ABYTES + BBYTES);
             tma_load_4d(sA + s * ABYTES, &mapA, &full[s], a.offx + kc * TC_BK, x0 + dx, y0 + dy, b);
             tma_load_2d(sB + s * BBYTES, &mapB, &full[s], tap * a.Cin + kc * TC_BK, n0);
+            n = it + 1;
         }
+        issued = n;
     } else if (warp == 1 && lane == 0) {  // MMA issuer
         constexpr uint32_t idesc = umma_idesc(TC_BM, BN);
         bool ok = true;
+        int n = 0;
         for (int it = 0; it < nk; ++it) {
             const int s = it % TC_ST;
             if (!mbar_wait(&full[s], (it / TC_ST) & 1)) { ok = false; break; }
+            n = it + 1;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const unsigned abase = tc_smem(sA + s * ABYTES), bbase = tc_smem(sB + s * BBYTES);
 #pragma unroll
@@ -193,6 +204,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3x3_tc(const __grid_constant
                 umma_f16(tmem, umma_desc(abase + 32 * k), umma_desc(bbase + 32 * k), idesc, (it | k) ? 1u : 0u);
             umma_commit(&empty[s]);  // the stage is free once these MMAs have read it
         }
+        consumed = n;
         if (!ok) failed = 1;
         umma_commit(&done);  // arrives when every MMA issued so far has completed
     }
@@ -201,6 +213,13 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3x3_tc(const __grid_constant
     const bool ready = mbar_wait(&done, 0);
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (!ready) failed = 1;
+    __syncthreads();
+    if (failed && threadIdx.x == 0) {
+        // Loads issued but never consumed may still be landing in this block's
+        // shared memory: wait for each (at most one per stage, since the producer
+        // waits for a stage to be freed before it reloads it).
+        for (int it = consumed; it < issued; ++it) mbar_wait(&full[it % TC_ST], (it / TC_ST) & 1);
+    }
     __syncthreads();
     const bool good = !failed;
     const int r = warp * 32 + lane;  // accumulator row = pixel of the block

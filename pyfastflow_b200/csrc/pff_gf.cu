@@ -244,7 +244,12 @@ static __device__ __align__(256) float g_fill_scratch[PFF_NOALLOC_MAX_CELLS];
 
 // Device address of g_fill_scratch per device, looked up once with that device
 // current (the host-side symbol is only a stand-in, not a device address).
-static float *g_fill_scratch_ptr[64] = {nullptr};
+// Atomic entries: host threads may make their first call concurrently; each
+// looks up the same address, so whichever store lands is correct.  The cached
+// address belongs to the device's current context: after cudaDeviceReset the
+// library's module is loaded again and the cache must not be trusted, so a
+// process that resets a device does not use this entry point afterwards.
+static std::atomic<float *> g_fill_scratch_ptr[64];
 
 static int fill_scratch_address(float **out)
 {
@@ -254,12 +259,14 @@ static int fill_scratch_address(float **out)
         set_error("pff_fill_z_add_delta_noalloc: device index %d out of range", dev);
         return PFF_ERR_ARG;
     }
-    if (!g_fill_scratch_ptr[dev]) {
+    float *ptr = g_fill_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!ptr) {
         void *p = nullptr;
         PFF_CUDA(cudaGetSymbolAddress(&p, g_fill_scratch));
-        g_fill_scratch_ptr[dev] = (float *)p;
+        ptr = (float *)p;
+        g_fill_scratch_ptr[dev].store(ptr, std::memory_order_release);
     }
-    *out = g_fill_scratch_ptr[dev];
+    *out = ptr;
     return PFF_OK;
 }
 

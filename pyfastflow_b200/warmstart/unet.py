@@ -48,6 +48,18 @@ def _call(name, *a):
     _lib.call(name, *a)
 
 
+def check_tensor_core_status():
+    """Raise PFFError if a tcgen05 convolution gave up waiting on its pipeline since
+    the last check (its outputs are then unspecified).  Synchronizes the device."""
+    import ctypes as C
+
+    flag = C.c_int()
+    _lib.call("pff_conv_tc_status", C.byref(flag))
+    if flag.value:
+        raise _lib.PFFError("a tcgen05 convolution timed out waiting on its TMA/MMA pipeline; "
+                            "its outputs are unspecified")
+
+
 class UNet:
     def __init__(self, seed: int = 0, device="cuda"):
         self.device = torch.device(device)
@@ -123,9 +135,11 @@ class UNet:
         return B, H >> lev, W >> lev
 
     # ---- forward ----------------------------------------------------------------------
-    def forward(self, x: torch.Tensor, B: int, H: int, W: int) -> torch.Tensor:
+    def forward(self, x: torch.Tensor, B: int, H: int, W: int, check: bool = True) -> torch.Tensor:
         """x: bf16 NHWC rows of 8 channels, B*H*W rows.  Returns pred (f32 rows of 8,
-        channel 0 = predicted log depth)."""
+        channel 0 = predicted log depth).  check: read the tensor-core error flag at
+        the end and raise if a convolution timed out (one device synchronisation;
+        pass False inside a training step whose backward() checks)."""
         self._alloc(B, H, W)
         st = _dev.stream()
         bf = self.buf
@@ -157,12 +171,15 @@ class UNet:
         conv(Ls["dec2a"]); conv(Ls["dec2b"]); up("d2", 128, "cat1", 2)
         conv(Ls["dec1a"]); conv(Ls["dec1b"]); up("d1", 64, "cat0", 1)
         conv(Ls["dec0a"]); conv(Ls["dec0b"]); conv(Ls["head"])
+        if check:
+            check_tensor_core_status()
         return bf["pred"]
 
     # ---- backward ---------------------------------------------------------------------
-    def backward(self, dpred: torch.Tensor):
+    def backward(self, dpred: torch.Tensor, check: bool = True):
         """dpred: bf16 rows of 8 (gradient of the loss w.r.t. pred).  Accumulates the
-        parameter gradients into self.g (zeroed here first)."""
+        parameter gradients into self.g (zeroed here first).  check: as in forward();
+        it covers every convolution since the last check, the forward pass's too."""
         st = _dev.stream()
         bf, gr = self.buf, self.grad
         self.g.zero_()
@@ -215,6 +232,8 @@ class UNet:
         pool_bwd("p0", "cat0", 64, 32, 0)
         conv_bwd("enc0b", "a0", 0)
         conv_bwd("enc0a", None, 0, need_dx=False)
+        if check:
+            check_tensor_core_status()
 
     def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, weight_decay=0.0):
         self.step_count += 1

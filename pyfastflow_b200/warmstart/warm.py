@@ -112,7 +112,7 @@ def train(net: UNet, x, tgt, side, weight=None, epochs=100, batch=16, lr=2e-3, s
             xb = x.view(ntiles, N * 8)[idx].reshape(-1)
             tb = tgt.view(ntiles, N)[idx].reshape(-1)
             wb = weight.view(ntiles, N)[idx].reshape(-1).contiguous() if weight is not None else None
-            net.forward(xb, batch, side, side)
+            net.forward(xb, batch, side, side, check=False)  # backward() checks the whole step
             loss, dp = net.loss_grad(tb, wb)
             net.backward(dp)
             cur_lr = lr * 0.5 * (1 + np.cos(np.pi * (ep * ntiles + s) / (epochs * ntiles)))

@@ -8,7 +8,7 @@ import types
 import pytest
 
 
-def fake_nvml(bits, fail=False):
+def fake_nvml(bits, fail=False, fail_after=None):
     m = types.ModuleType("pynvml")
     m.NVML_CLOCK_SM = 1
     m.nvmlInit = lambda: None
@@ -17,8 +17,11 @@ def fake_nvml(bits, fail=False):
     m.nvmlDeviceGetMaxClockInfo = lambda h, c: 1965
     m.nvmlDeviceGetClockInfo = lambda h, c: 1800
 
+    calls = [0]
+
     def reasons(h):
-        if fail:
+        calls[0] += 1
+        if fail or (fail_after is not None and calls[0] > fail_after):
             raise RuntimeError("query failed")
         return bits
 
@@ -49,3 +52,16 @@ def test_clock_query_failure_is_reported(monkeypatch):
         time.sleep(0.02)
     s = clk.summary()
     assert s["reasons"] == ["unsampled"] and "query failed" in s["error"]
+
+
+def test_clock_query_failure_after_samples_is_reported(monkeypatch):
+    """A query that fails part-way through the region: the samples taken before it are
+    kept, and the error is reported beside them (the reasons may be incomplete)."""
+    import bench
+
+    monkeypatch.setitem(sys.modules, "pynvml", fake_nvml(0x4, fail_after=3))
+    with bench.Clocks(0) as clk:
+        time.sleep(0.1)
+    s = clk.summary()
+    assert s["samples"] == 3 and s["reasons"] == ["sw_power_cap"]
+    assert "query failed" in s["error"]

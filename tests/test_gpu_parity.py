@@ -109,6 +109,31 @@ def test_basin_labels(orc, cuda, mode):
 
 
 @pytest.mark.parametrize("mode", MODES)
+def test_depression_counter(orc, cuda, mode):
+    """flow.depression_counter (lakeflow.py:25-44): interior self-receivers, on raw
+    receivers (many pits), on flats (ties give self-receivers) and after a reroute
+    (pits left only where the reference leaves them)."""
+    torch = cuda
+    from pyfastflow_b200 import flow
+
+    for kind, (nx, ny) in [("spectral", (203, 157)), ("int", (64, 48)), ("uniform", (9, 7))]:
+        g = Grid(orc, torch, nx, ny, mode, seed=5)
+        z = make_case(kind, nx, ny, seed=13 + mode)
+        set_constants(g, 10.0)
+        rcv, _ = orc.compute_receivers(z, g.og, 10.0)
+        want = orc.depression_counter(rcv, g.og)
+        assert flow.depression_counter(dev(torch, rcv)) == want, (kind, mode)
+        r2, _, _, _, _ = orc.reroute_flow(rcv, z, g.og)
+        assert flow.depression_counter(dev(torch, r2)) == orc.depression_counter(r2, g.og)
+    # a grid of one flat value: every cell is its own receiver; the count is the
+    # number of cells that cannot leave the domain
+    g = Grid(orc, torch, 16, 12, mode, seed=9)
+    set_constants(g, 1.0)
+    rcv = np.arange(g.N, dtype=np.int32)
+    assert flow.depression_counter(dev(torch, rcv)) == orc.depression_counter(rcv, g.og)
+
+
+@pytest.mark.parametrize("mode", MODES)
 def test_saddlesort(orc, cuda, mode):
     torch = cuda
     from pyfastflow_b200 import flow

@@ -1,6 +1,8 @@
 """Packed (f32, i32) key format, pinned by the reference's own checks in
 archive/test_pack_unpack.py (cases :16-26, ordering :68-77, seeded sort
-:175-230) -- the same scheme as pyfastflow/flow/f32_i32_struct.py."""
+:175-230) -- the same scheme as pyfastflow/flow/f32_i32_struct.py -- and by the
+atomic lexicographic argmin experiment archive/expe_lexicographic_argmin/t1.py
+:63-175 (an atomic min over packed keys is the (value, then index) argmin)."""
 import numpy as np
 
 from pyfastflow_b200.flow import f32_i32_struct as K
@@ -41,3 +43,30 @@ def test_signed_zero_and_invalid(orc):
     assert orc.pack_float_index(-0.0, 7) < orc.pack_float_index(0.0, 7)
     assert K.INVALID_KEY == orc.pack_float_index(1e8, 42)
     assert orc.unpack_float_index(K.INVALID_KEY) == (np.float32(1e8), 42)
+
+
+def test_atomic_min_is_lexicographic_argmin(orc):
+    """t1.py:63-175: 100 values uniform in [-100, 100) with indices 0..99, the value at
+    position 56 replaced by -99.5 with index 999; min over the packed keys must be
+    the manual lexicographic scan's (value, then index) winner.  Ties added at
+    both a larger and a smaller index check the index tie-break, which the saddle
+    pass's atomicMin (lakeflow.py:164-194) relies on."""
+    rng = np.random.default_rng(63)
+    vals = (rng.random(100) * 200.0 - 100.0).astype(np.float32)
+    idx = np.arange(100, dtype=np.int32)
+    vals[56], idx[56] = np.float32(-99.5), 999
+
+    def manual(v, ix):  # t1.py's verification loop
+        mv, mi = v[0], ix[0]
+        for a, b in zip(v[1:], ix[1:]):
+            if a < mv or (a == mv and b < mi):
+                mv, mi = a, b
+        return mv, mi
+
+    for extra in ([], [(np.float32(-99.5), 1200)], [(np.float32(-99.5), 7)], [(np.float32(-100.0), 3)]):
+        v = np.concatenate([vals, np.array([e[0] for e in extra], np.float32)])
+        ix = np.concatenate([idx, np.array([e[1] for e in extra], np.int32)])
+        keys = K.pack_float_index(v, ix)
+        got = K.unpack_float_index(int(keys.min()))
+        assert (np.float32(got[0]), int(got[1])) == manual(v, ix)
+        assert int(keys.min()) == min(orc.pack_float_index(a, int(b)) for a, b in zip(v, ix))

@@ -62,6 +62,15 @@ def test_noalloc_fill_matches_workspace_fill_twice(orc, cuda):
         for a, b in zip(ref, got):
             # the fill is deterministic: same IEEE operations in the same order
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        # and both equal the CPU oracle's fill (fill_topo.py:99-125, snapshot rounds) bit for bit
+        oz, oh, oz_ = orc.fill_z_add_delta(zh.copy(), h.copy(), rcv, 1e-3)
+        for want, have in ((oz, got[0]), (oh, got[1]), (oz_, got[2])):
+            assert np.array_equal(want.view(np.uint32), have.view(np.uint32))
+        # receivers_ after the rounds: the pointers jumped ceil(log2 N) times
+        jumped = rcv.copy()
+        for _ in range(orc.ceil_log2(rcv.size)):
+            jumped = jumped[jumped]
+        assert np.array_equal(got[3], jumped)
 
 
 def test_noalloc_fill_rejects_oversize_grid(cuda):

@@ -98,7 +98,7 @@ class Clocks:
                 sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
                 bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
                 self.rows.append((float(sm), float(mx), [k for k, b in self.REASONS.items() if bits & b]))
-                self.stop.wait(0.005)
+                self.stop.wait(0.002)
         except Exception as e:  # reported in the summary
             self.error = f"{type(e).__name__}: {e}"
 
@@ -107,6 +107,11 @@ class Clocks:
             nv, h = self._nvml_handle()
             self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
             self.t.start()
+            # the region starts once the sampler has its first row (at most 0.5 s):
+            # a short region must not end before the thread is scheduled
+            t0 = time.perf_counter()
+            while not self.rows and self.error is None and time.perf_counter() - t0 < 0.5:
+                time.sleep(0.001)
             return self
         except Exception as e:
             self.error = f"{type(e).__name__}: {e}"
@@ -469,7 +474,7 @@ def ragged_main(args):
         for fr in routers:
             fr.compute_receivers()
             fr.reroute_flow()
-            fr.accumulate_constant_Q(1.0, area=True)
+            fr.accumulate_constant_Q(1.0, area=True, exact_order=True)  # the batch's summation order
 
     per_tile()
     torch.cuda.synchronize()

@@ -102,6 +102,35 @@ int pff_accumulate_grid(const int32_t *receivers, float *Q, uint32_t *counts, in
  * results.  Process-wide; returns PFF_ERR_ARG for other values. */
 int pff_accumulate_set_front(int rounds);
 
+/* Drainage accumulation by hierarchical tile contraction, for any receiver forest
+ * (any in-degree: the jump rerouting of lakeflow.py:285-304, whose pits can gain
+ * more than 4 donors, is handled).  Replaces the whole accumulate_constant_Q chain
+ * of pyfastflow/flow/flowfields.py:254-292 (rcv2donor + rake_compress_accum + fuse,
+ * downstream_propag.py:21-179) with exact sums:
+ *   counts  out (optional): uint32 number of cells upstream of each cell, itself
+ *           included -- identical to the reference's counts;
+ *   Q       out (optional): the upstream sum of the seeds (weights[i], or `value`
+ *           for every cell if weights is NULL) formed exactly in 64-bit fixed point
+ *           (seed * 2^s, s chosen from max|seed| * N) and rounded once to f32.  The
+ *           reference's f32 sums carry their own rounding; Q differs from them by
+ *           that rounding only.  Seeds smaller than max|seed| * N * 2^-62 lose
+ *           their low bits.  Q may alias weights.  Deterministic.
+ *   local   1 if every receiver is the cell itself or a D4 neighbour (periodic
+ *           wrap included) -- the output of compute_receivers and of carve
+ *           rerouting; 0 for any receivers (each 32 x 32 tile may then have at most
+ *           256 cells whose receiver is outside it).
+ * Asynchronous (no host synchronisation).  Problems are recorded in a status word
+ * read by pff_accumulate_tree_status (synchronizes `stream`): 1 receiver out of
+ * range, 2 receiver cycle, 4 a tile with too many exits, 8 local = 1 violated,
+ * 16 non-finite seed; Q and counts are unspecified when it is nonzero.
+ * workspace: pff_accumulate_tree_workspace_bytes(nx, ny, local) bytes. */
+size_t pff_accumulate_tree_workspace_bytes(int nx, int ny, int local);
+int pff_accumulate_tree(const int32_t *receivers, const float *weights, float value, float *Q,
+                        uint32_t *counts, int nx, int ny, int local, void *workspace,
+                        size_t workspace_bytes, void *stream);
+int pff_accumulate_tree_status(int nx, int ny, int local, void *workspace, size_t workspace_bytes,
+                               int *status, void *stream);
+
 /* ---- lake / depression rerouting -----------------------------------------------
  * Replaces pyfastflow/flow/lakeflow.py:466-538 reroute_flow(bid, rec, rec_, rec__,
  * z, z_prime, is_border, outlet, basin_saddle, basin_saddlenode, tag, tag_,

@@ -30,6 +30,9 @@ SIGNATURES = {
     "pff_accumulate": (_i32, [_vp, _vp, _vp, _i32, _vp, _sz, _vp]),
     "pff_accumulate_grid": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _i32, _vp, _sz, _vp]),
     "pff_accumulate_set_front": (_i32, [_i32]),
+    "pff_accumulate_tree_workspace_bytes": (_sz, [_i32, _i32, _i32]),
+    "pff_accumulate_tree": (_i32, [_vp, _vp, _f32, _vp, _vp, _i32, _i32, _i32, _vp, _sz, _vp]),
+    "pff_accumulate_tree_status": (_i32, [_i32, _i32, _i32, _vp, _sz, C.POINTER(C.c_int), _vp]),
     "pff_reroute_workspace_bytes": (_sz, [_i32]),
     "pff_reroute_flow": (_i32, [_vp] * 12 + [_i32, _i32, _i32, _i32, _vp, _vp, _sz, C.POINTER(C.c_int), _vp]),
     "pff_basin_identification": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp]),

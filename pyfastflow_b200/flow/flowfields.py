@@ -68,6 +68,7 @@ class FlowRouter:
             self.tag_ = torch.zeros(N, dtype=torch.uint8, device=self.device)
             self.change = torch.zeros((), dtype=torch.uint8, device=self.device)
         self._ws_acc = _dev.Scratch()
+        self._ws_tree = _dev.Scratch()
         self._ws_lake = _dev.Scratch()
         self._ws_fill = _dev.Scratch()
         self._ws_diff = _dev.Scratch()
@@ -143,18 +144,58 @@ class FlowRouter:
                   self._codes(), wp, wn, C.byref(nout), _dev.stream())
         self.last_n_outer = nout.value
 
-    def _accumulate(self, counts: bool = True):
-        wp, wn = self._ws_acc.get(_lib.load().pff_accumulate_workspace_bytes(self.N), self.device)
+    def _accumulate(self, counts: bool = True, exact_order: bool = False, value=None):
+        """Upstream sums of the seeds (Q, or `value` per cell) into Q and counts.
+
+        Default: the tile-hierarchy accumulation (pff_accumulate_tree) -- exact
+        integer sums, Q rounded once to f32, exact counts.  exact_order=True, and
+        receivers the tree path reports it cannot take (a receiver cycle), use the
+        rake-and-compress rounds with the reference's f32 summation order
+        (pff_accumulate_grid), bit-identical to the reference's Q."""
+        lib = _lib.load()
+        if not exact_order:
+            import ctypes as C
+
+            local = 1
+            for _ in range(2):
+                wp, wn = self._ws_tree.get(lib.pff_accumulate_tree_workspace_bytes(self.nx, self.ny, local),
+                                           self.device)
+                seeds = None if value is not None else self.Q.data_ptr()
+                _lib.call("pff_accumulate_tree", self.receivers.data_ptr(), seeds,
+                          float(value) if value is not None else 0.0, self.Q.data_ptr(),
+                          self.counts.data_ptr() if counts else None, self.nx, self.ny, local, wp, wn,
+                          _dev.stream())
+                st = C.c_int()
+                _lib.call("pff_accumulate_tree_status", self.nx, self.ny, local, wp, wn, C.byref(st), _dev.stream())
+                if st.value == 0:
+                    return
+                if st.value & 1:
+                    raise _lib.PFFError("accumulate: a receiver index is out of range")
+                if st.value == 8 and local == 1:
+                    local = 0  # receivers that are not D4 neighbours (jump rerouting): general form
+                    continue
+                break
+            # a receiver cycle (or a tile with more than 256 outside receivers): the
+            # reference's own rounds, which define a result there
+            if value is not None:
+                self.Q.fill_(float(value))
+        wp, wn = self._ws_acc.get(lib.pff_accumulate_workspace_bytes(self.N), self.device)
         _lib.call("pff_accumulate_grid", self.receivers.data_ptr(), self.Q.data_ptr(),
                   self.counts.data_ptr() if counts else None, self.nx, self.ny, self.mode, self._codes(), self.N,
                   wp, wn, _dev.stream())
 
-    def accumulate_constant_Q(self, value, area=True, counts=True):
+    def accumulate_constant_Q(self, value, area=True, counts=True, exact_order=False):
         """flowfields.py:254-292: Q = value*dx^2 (area) or value per cell,
-        accumulated upstream.  Bit-identical to the reference's f32 result; the
-        exact uint32 upstream cell counts land in ``counts`` as well."""
-        self.Q.fill_(value * (self.dx * self.dx if area else 1.0))
-        self._accumulate(counts)
+        accumulated upstream; the exact uint32 upstream cell counts land in
+        ``counts``.  Q is the exact upstream sum rounded once to f32 (the
+        reference's f32 sums carry their own rounding); exact_order=True gives the
+        reference's f32 summation order bit for bit instead."""
+        v = value * (self.dx * self.dx if area else 1.0)
+        if exact_order:
+            self.Q.fill_(v)
+            self._accumulate(counts, exact_order=True)
+        else:
+            self._accumulate(counts, value=float(np.float32(v)))
 
     def route_many(self, dems, weights=None, out_Q=None, out_counts=None, carve=True):
         """Route a sequence of DEMs of this grid: for each k, z = dems[k] ->
@@ -234,12 +275,13 @@ class FlowRouter:
         main.wait_stream(d2h)
         main.wait_stream(h2d)
 
-    def accumulate_weighted_Q(self, weights, counts=True):
+    def accumulate_weighted_Q(self, weights, counts=True, exact_order=False):
         """Upstream sum of per-cell weights (e.g. precipitation-weighted
         discharge), the path scripts run by filling Q before rcv2donor
-        (examples/exemple_raw_1.py:135-150)."""
+        (examples/exemple_raw_1.py:135-150).  Exact sum rounded once to f32, or
+        the reference's f32 summation order with exact_order=True."""
         if isinstance(weights, torch.Tensor):
             self.Q.copy_(weights.reshape(-1).to(torch.float32))
         else:
             self.Q.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(weights, np.float32).ravel())))
-        self._accumulate(counts)
+        self._accumulate(counts, exact_order=exact_order)

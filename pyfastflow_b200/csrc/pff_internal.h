@@ -17,6 +17,10 @@ inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed);
 void set_error(const char *fmt, ...);
 void clear_error();
 
+// Internal status (never returned through the C ABI): a fast path that is not
+// available here, so the caller takes its general path.
+constexpr int PFF_ERR_UNSUPPORTED = 100;
+
 // Returns PFF_ERR_CUDA (and records where) if the last launch/copy failed.
 int check_cuda(const char *where);
 

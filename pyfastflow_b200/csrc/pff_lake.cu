@@ -11,6 +11,8 @@
 //     (k_saddle_p5_serial_fix).
 #include <cooperative_groups.h>
 #include <cstdlib>
+#include <cstring>
+#include <mutex>
 #include <cub/block/block_scan.cuh>
 #include "pff_internal.h"
 #include "pff_tiles.cuh"
@@ -44,10 +46,10 @@ __global__ void k_count_pits(const int32_t *__restrict__ rec, Grid g, int *count
 
 // basin_id_init (:47-61)
 template <int MODE>
-__global__ void k_basin_init(int32_t *bid, Grid g)
+__global__ void k_basin_init(int32_t *bid, Grid g, const int *guard)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.N()) return;
+    if (i >= g.N() || (guard && *guard == 0)) return;
     bid[i] = can_leave_i<MODE>(g, i) ? 0 : i + 1;
 }
 
@@ -312,21 +314,39 @@ __device__ __forceinline__ void block_append(bool pred, int val, int *list, int 
 
 // info[0] pits, info[2] set if some exit target is not a tile-border cell
 // (receivers that are not D4 neighbours)
-// tiles: optional list of tile ids (blockIdx.x indexes it) -- recompute only
-// those tiles; pits: optional (nullptr: no pit list).
+// tiles: optional list of tile ids -- recompute only those tiles; pits:
+// optional (nullptr: no pit list).
+template <int MODE>
+__device__ void tile_terminal_one(const int32_t *__restrict__ rec, int32_t *J, int32_t *R, int *pits, int *info,
+                                  const Grid &g, int tx, int ty, int *p, int *ext);
+
+// Tile terminals of the tiles listed in tiles[0 .. *ntiles) (one block per tile,
+// the grid strides over the list; the count is read on the device), or of every
+// tile (tiles == NULL, a 2-D grid of tiles).
 template <int MODE>
 __global__ void __launch_bounds__(TILE_THREADS) k_tile_terminal(const int32_t *__restrict__ rec, int32_t *J, int32_t *R,
-                                                                int *pits, int *info, Grid g, const int *tiles)
+                                                                int *pits, int *info, Grid g, const int *tiles,
+                                                                const int *ntiles)
 {
     __shared__ int p[TILE_CELLS];
     __shared__ int ext[TILE_CELLS];
-    const int nx = g.nx, ny = g.ny;
-    int tx = blockIdx.x, ty = blockIdx.y;
-    if (tiles) {
-        const int ntx = (nx + TILE_W - 1) / TILE_W, t = tiles[blockIdx.x];
-        ty = t / ntx;
-        tx = t - ty * ntx;
+    if (!tiles) {
+        tile_terminal_one<MODE>(rec, J, R, pits, info, g, blockIdx.x, blockIdx.y, p, ext);
+        return;
     }
+    const int ntx = (g.nx + TILE_W - 1) / TILE_W, n = *ntiles;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const int t = tiles[k];
+        tile_terminal_one<MODE>(rec, J, R, pits, info, g, t % ntx, t / ntx, p, ext);
+        __syncthreads();  // p and ext are reused by the next tile
+    }
+}
+
+template <int MODE>
+__device__ void tile_terminal_one(const int32_t *__restrict__ rec, int32_t *J, int32_t *R, int *pits, int *info,
+                                  const Grid &g, int tx, int ty, int *p, int *ext)
+{
+    const int nx = g.nx, ny = g.ny;
     const int col0 = tx * TILE_W, row0 = ty * TILE_H;
     const int w = min(TILE_W, nx - col0), h = min(TILE_H, ny - row0);
 #pragma unroll
@@ -991,8 +1011,10 @@ __global__ void k_dirty_list(uint8_t *dirty, int ntiles, int *list, int *count)
 // rec_ = rec on the carved cells: every write of the carve (reversed links and
 // saddle links) is at a tagged cell, and rec == rec_ everywhere else.
 __global__ void __launch_bounds__(256) k_sync_tagged(int32_t *rec_, const int32_t *__restrict__ rec,
-                                                     const uint8_t *__restrict__ tag, int N, int vec)
+                                                     const uint8_t *__restrict__ tag, int N, int vec,
+                                                     const int *guard)
 {
+    if (guard && *guard == 0) return;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = 4 * q;
     if (vec && i + 3 < N) {
@@ -1141,7 +1163,7 @@ static void l_count_pits(const int32_t *rec, const Grid &g, int *count, int *lis
 template <int MODE>
 static void l_basin_init(int32_t *bid, const Grid &g, cudaStream_t st)
 {
-    { k_basin_init<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(bid, g); count_launch(); }
+    { k_basin_init<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(bid, g, nullptr); count_launch(); }
 }
 template <int MODE>
 static void l_saddle(const int32_t *bid, uint8_t *isb, float *zp, long long *saddle, int32_t *snode,
@@ -1163,14 +1185,13 @@ static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pit
                             cudaStream_t st)
 {
     dim3 gr(div_up(g.nx, TILE_W), div_up(g.ny, TILE_H));
-    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g, nullptr); count_launch(); }
+    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g, nullptr, nullptr); count_launch(); }
 }
 template <int MODE>
 static void l_tile_terminal_list(const int32_t *rec, int32_t *J, int32_t *R, int *info, const Grid &g,
-                                 const int *tiles, int ntiles, cudaStream_t st)
+                                 const int *tiles, const int *ntiles, int grid, cudaStream_t st)
 {
-    if (ntiles <= 0) return;
-    { k_tile_terminal<MODE><<<ntiles, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles); count_launch(); }
+    { k_tile_terminal<MODE><<<grid, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles, ntiles); count_launch(); }
 }
 template <int MODE>
 static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, const int32_t *rec,
@@ -1204,6 +1225,12 @@ static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long lon
     { k_saddle_p5_decide_list<<<grid, 256, 0, st>>>(bid, outlet, inv, N, pits, np); count_launch(); }
     { k_saddle_p5_serial_fix<<<1, 32, 0, st>>>(bid, outlet, inv, N); count_launch(); }
     { k_saddle_p5_apply_list<<<grid, 256, 0, st>>>(saddle, outlet, snode, inv, N, pits, np); count_launch(); }
+}
+
+template <int MODE>
+static void l_basin_init_if(int32_t *bid, const Grid &g, const int *guard, cudaStream_t st)
+{
+    { k_basin_init<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(bid, g, guard); count_launch(); }
 }
 
 int launch_basin_init(int32_t *bid, const Grid &g, cudaStream_t st)
@@ -1397,52 +1424,426 @@ static int general_labels(const int32_t *rec, int32_t *work, int32_t *bid, const
 
 }  // namespace pff
 
-extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
-                                float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
-                                int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int carve, int nx, int ny,
-                                int bound_mode, const uint8_t *codes, void *workspace, size_t workspace_bytes,
-                                int *n_outer_out, void *stream)
+namespace pff {
+// ---- the outer loop of reroute_flow driven on the device (carve rerouting) -------------
+// The host-driven loop reads pit counts and flags once per outer iteration to
+// decide whether to go on.  Here the decisions are made by one-thread kernels
+// that set CUDA-graph conditional handles, so a whole call is one graph launch:
+//
+//   prologue: rec_ = rec, counters zeroed, tile terminals + pit list
+//   plan0 (IF pits and D4 receivers):
+//     labels by border pointer jumping; plan1 (IF no receiver cycle):
+//       iteration 0 (strip saddle pass, carve, relabel preparation); decide
+//       WHILE (go on): iteration (parity 1); decide; IF (go on): iteration (parity 0); decide
+//   basin_id_init (:537) when the loop ended normally
+//
+// Two iterations per WHILE body keep every kernel argument fixed (the list
+// buffers alternate with the iteration's parity).  decide mirrors the host loop's
+// tests in its order (:500, :512-514 and the carve checks) and stops the loop
+// after at most outer <= 32 iterations.  The rare cases that need the
+// reference's N-wide steps (non-D4 receivers, receiver cycles) stop the graph in
+// a recorded state; the host then runs those steps from there.
+//
+// ctl = w.ctr + RR_CTL: [0] iteration, [1] outer, [2] n_outer, [3] state,
+// [4] sync_tagged needed, [5] basin_init needed, [6] plan0 passed, [7] plan1
+// passed, [8] iterations run.
+enum { RR_RUN = 0, RR_NOPITS = 1, RR_DONE = 2, RR_GENERAL = 3, RR_RESUME = 4, RR_WALKERR = 5, RR_BOUND = 6 };
+constexpr int RR_CTL = 400;
+
+__device__ __forceinline__ int d_ceil_log2(long long n)
 {
-    clear_error();
-    PFF_TRY(check_grid(nx, ny, bound_mode, codes));
-    if (!bid || !rec || !rec_ || !rec__ || !z || !z_prime || !is_border || !outlet || !basin_saddle ||
-        !basin_saddlenode || !tag || !tag_) {
-        set_error("pff_reroute_flow: null pointer");
-        return PFF_ERR_ARG;
+    int r = 0;
+    long long p = 1;
+    while (p < n) { p <<= 1; ++r; }
+    return r;
+}
+
+__global__ void k_rr_plan0(int *ctl, const int *info, cudaGraphConditionalHandle ha)
+{
+    if (threadIdx.x) return;
+    const int npits = info[0], nonlocal = info[2];
+    for (int k = 0; k < 9; ++k) ctl[k] = 0;
+    int go = 0;
+    if (npits == 0) ctl[3] = RR_NOPITS;                 // :496-497
+    else {
+        ctl[1] = d_ceil_log2(npits) + 1;                // :500
+        if (nonlocal) ctl[3] = RR_GENERAL;
+        else { ctl[3] = RR_RUN; go = 1; }
     }
-    const int N = nx * ny;
-    if (!workspace || workspace_bytes < pff_reroute_workspace_bytes(N)) {
-        set_error("pff_reroute_flow: workspace too small");
-        return PFF_ERR_WORKSPACE;
+    ctl[6] = go;
+    cudaGraphSetConditional(ha, go);
+}
+
+__global__ void k_rr_plan1(int *ctl, const int *unresolved, cudaGraphConditionalHandle hb)
+{
+    if (threadIdx.x) return;
+    const int go = *unresolved ? 0 : 1;
+    if (!go) ctl[3] = RR_GENERAL;  // the input receivers hold a cycle
+    ctl[7] = go;
+    cudaGraphSetConditional(hb, go);
+}
+
+__global__ void k_rr_decide(int *ctl, const int *ctr, const int *np_next, cudaGraphConditionalHandle hc,
+                            cudaGraphConditionalHandle hm, int set_hm)
+{
+    if (threadIdx.x) return;
+    const int it = ctl[0], outer = ctl[1];
+    int n_outer = ctl[2] + 1;
+    const int walk_err = ctr[43], odd = ctr[45], cycle = ctr[49], nd_next = *np_next;
+    int state = RR_RUN;
+    if (walk_err) state = RR_WALKERR;
+    else if (odd) state = RR_RESUME;              // a reversed path without an outlet link
+    else if (it + 1 >= outer) state = RR_DONE;    // :500
+    else if (cycle) state = RR_RESUME;            // the carve closed a receiver cycle
+    else if (nd_next == 0) { ++n_outer; state = RR_DONE; }  // the next count is 0 (:512-514)
+    else if (it + 1 >= 64) state = RR_BOUND;
+    ctl[2] = n_outer;
+    ctl[3] = state;
+    ctl[4] = state != RR_RUN;                     // rec_ = rec on the carved cells before stopping
+    ctl[5] = state == RR_DONE || state == RR_WALKERR;
+    ctl[8] += 1;
+    if (state == RR_RUN) ctl[0] = it + 1;
+    cudaGraphSetConditional(hc, state == RR_RUN);
+    if (set_hm) cudaGraphSetConditional(hm, state == RR_RUN);
+}
+
+struct RRBufs {
+    int32_t *bid, *rec, *rec_, *rec__;
+    const float *z;
+    float *zp;
+    uint8_t *isb;
+    long long *out, *sad;
+    int32_t *snode;
+    uint8_t *tag, *tag_;
+    Grid g;
+    RerouteWs w;
+};
+
+static int coop_blocks_for(const void *fn)
+{
+    int dev = 0, nsm = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 256, 0);
+    return nsm * (per < 4 ? per : 4);
+}
+
+// One fast outer iteration with list parity par, enqueued on s (captured).  first:
+// iteration 0 (labels come from the prologue); otherwise it starts with the basin
+// relabelling and the dirty tiles' terminals that the previous iteration's
+// decision asked for.
+static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
+{
+    const Grid &g = A.g;
+    const RerouteWs &w = A.w;
+    const int N = g.N(), nx = g.nx, B = 256;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = nsm * 8;
+    const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(g.ny, TILE_H);
+    int *np = w.ctr + 16 * par, *np_next = w.ctr + 16 * (par ^ 1);
+    if (!first) {
+        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, s>>>(A.bid, w.fin, A.rec_, A.rec, A.tag, N,
+                                                         ((uintptr_t)A.bid & 15) == 0 && ((uintptr_t)A.tag & 3) == 0); count_launch(); }
+        PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, A.rec_, A.rec__, w.R, np_next, g, w.tiles, w.ctr + 44,
+                          std::min(ntiles, grid), s);
+        { k_basin_reset_list<<<grid, B, 0, s>>>(A.sad, A.out, A.snode, w.inv, w.pits[par ^ 1], np_next); count_launch(); }
+    } else {
+        { k_basin_arrays_init<<<div_up(N + 1, B), B, 0, s>>>(A.sad, A.out, A.snode, w.inv, N + 1); count_launch(); }
     }
-    Grid g{nx, ny, bound_mode, codes};
-    cudaStream_t st = S(stream);
-    RerouteWs w = carve_ws(workspace, workspace_bytes, N);
-    long long *sad = (long long *)basin_saddle, *out = (long long *)outlet;
+    PFF_CUDA(cudaMemsetAsync(w.ctr + 40, 0, 6 * sizeof(int), s));
+    PFF_CUDA(cudaMemsetAsync(w.ctr + 50 + par, 0, sizeof(int), s));
+    PFF_MODE_DISPATCH(g.mode, l_saddle_lists, A.bid, A.isb, A.zp, A.sad, A.snode, A.out, w.inv, A.z, g, w.pits[par],
+                      np, w.blist, w.ctr + 40, first ? nullptr : w.alist[par ^ 1], w.ctr + 50 + (par ^ 1),
+                      w.alist[par], w.ctr + 50 + par, grid, s);
+    PFF_CUDA(cudaMemsetAsync(A.tag, 0, (size_t)N, s));
+    PFF_CUDA(cudaMemsetAsync(A.tag_, 0, (size_t)N, s));
+    { k_carve_segments<<<nsm * 4, 32 * SEG_WARPS, 0, s>>>(A.snode, A.rec_, A.rec__, w.pits[par], np, N, w.segs,
+                                                           w.ctr + 41, N, w.ctr + 43); count_launch(); }
+    { k_carve_walk<<<nsm * 4, WALK_THREADS, 0, s>>>(A.rec_, A.rec, A.tag, A.tag_, w.segs, w.ctr + 41, N, nx, g.ny,
+                                                     w.dirty); count_launch(); }
+    { k_carve_link_list<<<grid, B, 0, s>>>(A.rec, A.snode, A.out, w.pits[par], np, N, w.dirty, nx); count_launch(); }
+    PFF_CUDA(cudaMemsetAsync(np_next, 0, 4 * sizeof(int), s));
+    { k_relabel_init<<<grid, B, 0, s>>>(w.fin, A.bid, A.snode, A.out, w.pits[par], np, N, w.pits[par ^ 1], np_next,
+                                        w.ctr + 45); count_launch(); }
+    { k_dirty_list<<<div_up(ntiles, B), B, 0, s>>>(w.dirty, ntiles, w.tiles, w.ctr + 44); count_launch(); }
+    int *flags = w.ctr + 256;
+    PFF_CUDA(cudaMemsetAsync(flags, 0, 64 * sizeof(int), s));
+    static int coop_relabel = 0;
+    if (!coop_relabel) coop_relabel = coop_blocks_for((const void *)k_relabel_jump_coop);
+    int *plist = w.pits[par];
+    int32_t *fin = w.fin;
+    void *args[] = {&fin, &plist, &np, &flags};
+    PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, s));
+    count_launch();
+    PFF_CUDA(cudaMemsetAsync(w.ctr + 49, 0, sizeof(int), s));
+    { k_relabel_check<<<grid, B, 0, s>>>(w.fin, A.out, w.pits[par], np, N, w.ctr + 49); count_launch(); }
+    return check_cuda("reroute iteration");
+}
+
+// streams used to capture the graph's nested bodies (one per nesting depth)
+static cudaStream_t rr_capture_stream(int dev, int depth)
+{
+    static cudaStream_t streams[64][5];
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!streams[dev][depth]) cudaStreamCreateWithFlags(&streams[dev][depth], cudaStreamNonBlocking);
+    return streams[dev][depth];
+}
+
+// a conditional node after the current capture frontier of s; its body graph is returned
+static int rr_cond(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t *body)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t gr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    PFF_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &gr, &deps, &nd));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    PFF_CUDA(cudaGraphAddNode(&node, gr, deps, nd, &p));
+    *body = p.conditional.phGraph_out[0];
+    PFF_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return PFF_OK;
+}
+
+static int rr_handle(cudaStream_t s, cudaGraphConditionalHandle *h)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t gr;
+    PFF_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &gr, nullptr, nullptr));
+    PFF_CUDA(cudaGraphConditionalHandleCreate(h, gr, 0, cudaGraphCondAssignDefault));
+    return PFF_OK;
+}
+
+struct RRKernelCounts {
+    long long pro, a, b0, it2;  // kernels in the prologue, body A, iteration 0, a parity-1 iteration + decide
+};
+
+// Capture the whole graph.  Every capture begun here is ended on every path.
+static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *kc)
+{
+    const Grid &g = A.g;
+    const RerouteWs &w = A.w;
+    const int N = g.N();
+    const size_t nb4 = sizeof(int32_t) * (size_t)N;
+    const int ntx = div_up(g.nx, TILE_W), ntiles = ntx * div_up(g.ny, TILE_H);
+    int *ctl = w.ctr + RR_CTL;
+    cudaStream_t s[5];
+    for (int d = 0; d < 5; ++d) {
+        s[d] = rr_capture_stream(dev, d);
+        if (!s[d]) { set_error("reroute graph: no capture stream"); return PFF_ERR_CUDA; }
+    }
+    int depth = 0, rc = PFF_OK;
+    cudaGraph_t body[5] = {G, nullptr, nullptr, nullptr, nullptr};
+    auto begin = [&](int d) -> int {
+        PFF_CUDA(cudaStreamBeginCaptureToGraph(s[d], body[d], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        depth = d + 1;
+        return PFF_OK;
+    };
+    long long l0 = g_launches.load();
+    do {
+        if ((rc = begin(0))) break;
+        // prologue (:491)
+        if (cudaMemcpyAsync(A.rec_, A.rec, nb4, cudaMemcpyDeviceToDevice, s[0]) != cudaSuccess ||
+            cudaMemsetAsync(w.ctr, 0, 512 * sizeof(int), s[0]) != cudaSuccess ||
+            cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, s[0]) != cudaSuccess) { rc = check_cuda("reroute graph"); break; }
+        PFF_MODE_DISPATCH(g.mode, l_tile_terminal, A.rec_, A.rec__, w.R, w.pits[0], w.ctr, g, s[0]);
+        cudaGraphConditionalHandle ha, hb, hc, hm;
+        if ((rc = rr_handle(s[0], &ha))) break;
+        { k_rr_plan0<<<1, 32, 0, s[0]>>>(ctl, w.ctr, ha); count_launch(); }
+        kc->pro = g_launches.load() - l0;
+        l0 = g_launches.load();
+        if ((rc = rr_cond(s[0], ha, cudaGraphCondTypeIf, &body[1]))) break;
+        if ((rc = begin(1))) break;
+        // labels: pointer jumping over border cells, one gather per cell
+        if (cudaMemsetAsync(w.ctr + 64, 0, 64 * sizeof(int), s[1]) != cudaSuccess ||
+            cudaMemsetAsync(w.ctr + 48, 0, sizeof(int), s[1]) != cudaSuccess) { rc = check_cuda("reroute graph"); break; }
+        {
+            static int coop_border = 0;
+            if (!coop_border) coop_border = coop_blocks_for((const void *)k_border_jump_coop);
+            int nx = g.nx, ny = g.ny, tx = ntx;
+            long long nslots = (long long)ntx * div_up(g.ny, TILE_H) * BORDER_SLOTS;
+            int32_t *R = w.R;
+            int *flags = w.ctr + 64;
+            void *args[] = {&R, &nx, &ny, &tx, &nslots, &flags};
+            if (cudaLaunchCooperativeKernel((void *)k_border_jump_coop, coop_border, 256, args, 0, s[1]) != cudaSuccess) {
+                rc = check_cuda("reroute graph: cooperative launch");
+                break;
+            }
+            count_launch();
+        }
+        PFF_MODE_DISPATCH(g.mode, l_labels_final, A.rec__, w.R, A.bid, g, A.rec_, w.ctr + 48, s[1]);
+        if ((rc = rr_handle(s[1], &hb))) break;
+        { k_rr_plan1<<<1, 32, 0, s[1]>>>(ctl, w.ctr + 48, hb); count_launch(); }
+        kc->a = g_launches.load() - l0;
+        l0 = g_launches.load();
+        if ((rc = rr_cond(s[1], hb, cudaGraphCondTypeIf, &body[2]))) break;
+        if ((rc = begin(2))) break;
+        if ((rc = rr_iteration(A, 0, true, s[2]))) break;
+        if ((rc = rr_handle(s[2], &hc))) break;
+        { k_rr_decide<<<1, 32, 0, s[2]>>>(ctl, w.ctr, w.ctr + 16, hc, hc, 0); count_launch(); }
+        { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[2]>>>(A.rec_, A.rec, A.tag, N,
+                                                                   ((uintptr_t)A.tag & 3) == 0, ctl + 4); count_launch(); }
+        kc->b0 = g_launches.load() - l0;
+        l0 = g_launches.load();
+        if ((rc = rr_cond(s[2], hc, cudaGraphCondTypeWhile, &body[3]))) break;
+        if ((rc = begin(3))) break;
+        if ((rc = rr_iteration(A, 1, false, s[3]))) break;
+        if ((rc = rr_handle(s[3], &hm))) break;
+        { k_rr_decide<<<1, 32, 0, s[3]>>>(ctl, w.ctr, w.ctr, hc, hm, 1); count_launch(); }
+        { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[3]>>>(A.rec_, A.rec, A.tag, N,
+                                                                   ((uintptr_t)A.tag & 3) == 0, ctl + 4); count_launch(); }
+        kc->it2 = g_launches.load() - l0;
+        if ((rc = rr_cond(s[3], hm, cudaGraphCondTypeIf, &body[4]))) break;
+        if ((rc = begin(4))) break;
+        if ((rc = rr_iteration(A, 0, false, s[4]))) break;
+        { k_rr_decide<<<1, 32, 0, s[4]>>>(ctl, w.ctr, w.ctr + 16, hc, hc, 0); count_launch(); }
+        { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[4]>>>(A.rec_, A.rec, A.tag, N,
+                                                                   ((uintptr_t)A.tag & 3) == 0, ctl + 4); count_launch(); }
+        // close the bodies, innermost first; then basin_id_init on the top level
+        for (int d = 4; d >= 1; --d) {
+            cudaGraph_t out_g;
+            if (cudaStreamEndCapture(s[d], &out_g) != cudaSuccess) { rc = check_cuda("reroute graph: end capture"); break; }
+            depth = d;
+        }
+        if (rc) break;
+        PFF_MODE_DISPATCH(g.mode, l_basin_init_if, A.bid, g, ctl + 5, s[0]);
+    } while (0);
+    // end every capture still open (innermost first)
+    for (int d = depth - 1; d >= 0; --d) {
+        cudaGraph_t out_g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s[d], &out_g);
+        if (e != cudaSuccess && rc == PFF_OK) {
+            set_error("reroute graph: end capture: %s", cudaGetErrorString(e));
+            rc = PFF_ERR_CUDA;
+        }
+    }
+    cudaGetLastError();
+    return rc;
+}
+
+// every pointer and size the graph bakes in, as plain 64-bit words (no padding)
+struct RRKey {
+    unsigned long long v[32];
+    int n = 0;
+    void add(unsigned long long x) { v[n++] = x; }
+    void add(const void *p) { v[n++] = (unsigned long long)(uintptr_t)p; }
+    bool operator==(const RRKey &o) const { return n == o.n && std::memcmp(v, o.v, sizeof(v[0]) * n) == 0; }
+};
+struct RREntry {
+    RRKey key;
+    cudaGraphExec_t exec = nullptr;
+    RRKernelCounts kc{};
+};
+
+// Launch the device-driven loop for these buffers (a graph built and kept on the
+// first call with them), then read its final state (one synchronisation).
+// Returns PFF_ERR_UNSUPPORTED when graphs cannot be built here.
+static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z, float *z_prime,
+                         uint8_t *is_border, long long *out, long long *sad, int32_t *snode, uint8_t *tag,
+                         uint8_t *tag_, const Grid &g, RerouteWs &w, void *workspace, size_t workspace_bytes,
+                         int *state, int *it, int *outer, int *n_outer, cudaStream_t st)
+{
+    static std::mutex mu;
+    static RREntry cache[8];
+    static int next = 0;
+    static bool disabled = getenv("PFF_REROUTE_NO_GRAPH") != nullptr;  // diagnostics: force the host loop
+    if (disabled) return PFF_ERR_UNSUPPORTED;
+    (void)workspace;
+    (void)workspace_bytes;
+    int dev = 0;
+    PFF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return PFF_ERR_UNSUPPORTED;
+    const RRBufs bufs{bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, snode, tag, tag_, g, w};
+    RRKey key;
+    for (const void *p : {(const void *)bid, (const void *)rec, (const void *)rec_, (const void *)rec__,
+                          (const void *)z, (const void *)z_prime, (const void *)is_border, (const void *)out,
+                          (const void *)sad, (const void *)snode, (const void *)tag, (const void *)tag_,
+                          (const void *)g.codes, (const void *)w.inv, (const void *)w.ctr})
+        key.add(p);
+    key.add((unsigned long long)g.nx);
+    key.add((unsigned long long)g.ny);
+    key.add((unsigned long long)g.mode);
+    key.add((unsigned long long)dev);
+    cudaGraphExec_t exec = nullptr;
+    RRKernelCounts kc{};
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto &e : cache)
+            if (e.exec && e.key == key) { exec = e.exec; kc = e.kc; }
+        if (!exec) {
+            cudaGraph_t G = nullptr;
+            PFF_CUDA(cudaGraphCreate(&G, 0));
+            const long long l0 = g_launches.load();
+            int rc = rr_capture(bufs, dev, G, &kc);
+            g_launches.store(l0);  // captured, not launched: replays are counted below
+            if (rc == PFF_OK && cudaGraphInstantiate(&exec, G, 0) != cudaSuccess) {
+                set_error("reroute graph: instantiate: %s", cudaGetErrorString(cudaGetLastError()));
+                exec = nullptr;
+                rc = PFF_ERR_UNSUPPORTED;
+            }
+            cudaGraphDestroy(G);
+            if (rc != PFF_OK) {
+                cudaGetLastError();
+                return PFF_ERR_UNSUPPORTED;
+            }
+            RREntry &e = cache[next];
+            next = (next + 1) % 8;
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+            e.key = key;
+            e.exec = exec;
+            e.kc = kc;
+        }
+    }
+    PFF_CUDA(cudaGraphLaunch(exec, st));
+    int c[9];
+    PFF_TRY(read_ints(IntReads().add(w.ctr + RR_CTL, 9), c, st));
+    *it = c[0];
+    *outer = c[1];
+    *n_outer = c[2];
+    *state = c[3];
+    // kernels this launch ran: prologue, body A, iteration 0, then the iterations of the WHILE
+    long long nk = kc.pro;
+    if (c[6]) nk += kc.a;
+    if (c[7] && c[8] > 0) nk += kc.b0 + (long long)(c[8] - 1) * kc.it2;
+    g_launches.fetch_add(nk + (c[5] ? 1 : 0));  // + basin_id_init
+    return check_cuda("reroute graph launch");
+}
+
+// The outer loop of reroute_flow driven from the host, from iteration it_start
+// (0: from the start; else resuming after a device-driven iteration, in general
+// mode, with outer and n_outer as they were).  Ends with basin_id_init (:537) and
+// the error checks.
+static int reroute_host_loop(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                             float *z_prime, uint8_t *is_border, long long *out, long long *sad,
+                             int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int carve, const Grid &g,
+                             RerouteWs &w, int it_start, int outer, bool general, int n_outer, int *n_outer_out,
+                             cudaStream_t st)
+{
+    const int N = g.N(), nx = g.nx, bound_mode = g.mode;
     const size_t nb4 = sizeof(int32_t) * (size_t)N;
     const int B = 256, nbk = div_up(N, B);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = nsm * 8;
-    if (n_outer_out) *n_outer_out = 0;
-
-    PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :491
-    PFF_CUDA(cudaMemsetAsync(w.ctr, 0, 512 * sizeof(int), st));
-    const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(ny, TILE_H);
-    PFF_CUDA(cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, st));
-    int outer = 0, n_outer = 0;
+    const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(g.ny, TILE_H);
     // Fast mode (carve, D4 receivers, no receiver cycle): tile labels in the first
     // iteration, basin relabelling and dirty-tile terminals afterwards, list-driven
     // saddle passes, tile-walk carving.  General mode (jump rerouting, non-D4
     // receivers, or once a receiver cycle appears): the reference's own steps with
     // its serial semantics, N-wide.
-    bool general = !carve;
     bool incremental = false;
     int nd_next = 0;
     int *cyc_err = w.ctr + 47;
     static const bool trace = getenv("PFF_TRACE_REROUTE") != nullptr;  // diagnostic trace on stderr
-    for (int it = 0;; ++it) {
+    for (int it = it_start;; ++it) {
         if (it > 0 && it >= outer) break;  // :500
         const int par = it & 1;
         int *np = w.ctr + 16 * par;
@@ -1564,7 +1965,7 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         // rec_ = rec on the carved cells (:526): inside the relabelling pass when
         // the loop goes on, else here
         if (h[0] || h[2] || it + 1 >= outer || hc || nd_next == 0) {
-            { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0); count_launch(); }
+            { k_sync_tagged<<<div_up(div_up(N, 4), B), B, 0, st>>>(rec_, rec, tag, N, ((uintptr_t)tag & 3) == 0, nullptr); count_launch(); }
         }
         if (h[0]) break;  // walk bounds exceeded: reported below
         const int ndirty = h[1];
@@ -1585,7 +1986,9 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         }
         { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, rec_, rec, tag, N,
                                                            ((uintptr_t)bid & 15) == 0 && ((uintptr_t)tag & 3) == 0); count_launch(); }
-        PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, ndirty, st);
+        if (ndirty > 0)
+            PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, w.ctr + 44,
+                              std::min(ndirty, nsm * 8), st);
         incremental = true;
         PFF_TRY(check_cuda("pff_reroute_flow"));
     }
@@ -1603,4 +2006,64 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
     }
     if (n_outer_out) *n_outer_out = n_outer;
     return check_cuda("pff_reroute_flow");
+}
+
+}  // namespace pff
+
+extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                                float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
+                                int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int carve, int nx, int ny,
+                                int bound_mode, const uint8_t *codes, void *workspace, size_t workspace_bytes,
+                                int *n_outer_out, void *stream)
+{
+    clear_error();
+    PFF_TRY(check_grid(nx, ny, bound_mode, codes));
+    if (!bid || !rec || !rec_ || !rec__ || !z || !z_prime || !is_border || !outlet || !basin_saddle ||
+        !basin_saddlenode || !tag || !tag_) {
+        set_error("pff_reroute_flow: null pointer");
+        return PFF_ERR_ARG;
+    }
+    const int N = nx * ny;
+    if (!workspace || workspace_bytes < pff_reroute_workspace_bytes(N)) {
+        set_error("pff_reroute_flow: workspace too small");
+        return PFF_ERR_WORKSPACE;
+    }
+    Grid g{nx, ny, bound_mode, codes};
+    cudaStream_t st = S(stream);
+    RerouteWs w = carve_ws(workspace, workspace_bytes, N);
+    long long *sad = (long long *)basin_saddle, *out = (long long *)outlet;
+    const size_t nb4 = sizeof(int32_t) * (size_t)N;
+    if (n_outer_out) *n_outer_out = 0;
+    if (carve) {
+        int state = 0, it = 0, outer = 0, n_outer = 0;
+        const int rc = reroute_graph(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag,
+                                     tag_, g, w, workspace, workspace_bytes, &state, &it, &outer, &n_outer, st);
+        if (rc == PFF_OK) {
+            if (state == RR_NOPITS) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
+            if (state == RR_GENERAL)  // non-D4 receivers or a receiver cycle in the input: the reference's steps
+                return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode,
+                                         tag, tag_, carve, g, w, 0, 0, true, 0, n_outer_out, st);
+            if (state == RR_RESUME)  // the carve closed a receiver cycle: the reference's steps from here on
+                return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode,
+                                         tag, tag_, carve, g, w, it + 1, outer, true, n_outer, n_outer_out, st);
+            if (state == RR_WALKERR) {
+                set_error("pff_reroute_flow: carve walk exceeded its bounds");
+                return PFF_ERR_NOCONV;
+            }
+            if (state != RR_DONE) {
+                set_error("pff_reroute_flow: outer loop ended in state %d", state);
+                return PFF_ERR_NOCONV;
+            }
+            if (n_outer_out) *n_outer_out = n_outer;
+            return check_cuda("pff_reroute_flow");
+        }
+        if (rc != PFF_ERR_UNSUPPORTED) return rc;
+        clear_error();  // graphs unavailable: the host-driven loop below
+    }
+    PFF_CUDA(cudaMemcpyAsync(rec_, rec, nb4, cudaMemcpyDeviceToDevice, st));  // :491
+    PFF_CUDA(cudaMemsetAsync(w.ctr, 0, 512 * sizeof(int), st));
+    const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(ny, TILE_H);
+    PFF_CUDA(cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, st));
+    return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag, tag_,
+                             carve, g, w, 0, 0, !carve, 0, n_outer_out, st);
 }

@@ -221,6 +221,33 @@ int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, cons
  * reference counterpart. */
 int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *stream);
 
+/* ---- legacy downstream tree algorithms (pyfastflow's archive) ----------------------
+ * The kernels of archive/fastflow/kernels with the drivers of
+ * archive/_save_fasftflow/fastflow: ceil(log2 N) pointer-jumping rounds, each
+ * reading the start-of-round arrays.  rcv, W and p are updated in place as those
+ * drivers leave them (rcv jumped).  Synchronize `stream` (a receiver range check).
+ *   pff_tree_accum_down  tree_accum_down.py:15-21: p = p + W*p[rcv], W = W*W[rcv],
+ *                        rcv = rcv[rcv] -- solves x = p + W*x[rcv] downstream;
+ *   pff_tree_max_down    tree_max_down.py:7-12: where rcv[rcv] != rcv,
+ *                        p = max(p[rcv], p), rcv = rcv[rcv] -- the largest value on
+ *                        the downstream path, the final root's value excluded;
+ *                        max(a, b) = a > b ? a : b;
+ *   pff_erode_deposit    erode_deposit.py:7-24 then _archived/erode_deposit.py:30-39:
+ *                        z += dt*min(k_d/drain, 1)*Qs off the boundary (bound != 0),
+ *                        K = dt/dx*(k_spl*drain^m + k_t + k_h*drain^-m),
+ *                        pe = z/(1+K), We = K/(1+K) (pe = z, We = 0 on the boundary),
+ *                        then tree_accum_down(rcv, We, pe): pe ends as the new
+ *                        elevations.  Powers are evaluated in double and rounded
+ *                        once to f32.
+ * workspace: pff_archive_workspace_bytes(N). */
+size_t pff_archive_workspace_bytes(int N);
+int pff_tree_accum_down(int32_t *rcv, float *W, float *p, int N, void *workspace, size_t workspace_bytes,
+                        void *stream);
+int pff_tree_max_down(int32_t *rcv, float *p, int N, void *workspace, size_t workspace_bytes, void *stream);
+int pff_erode_deposit(float *z, const uint8_t *bound, int32_t *rcv, const float *drain, const float *Qs,
+                      float dt, float dx, float k_spl, float k_t, float k_h, float k_d, float m, float *pe,
+                      float *We, int N, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- Ragged batch ----------------------------------------------------------------
  * Many independent tiles (own nx, ny, dx, boundary mode 0-3) packed back to back,
  * tile t's cells at [tile_offset[t], tile_offset[t] + nx*ny) in row-major order.

@@ -69,6 +69,10 @@ def lib():
         _lib.orc_count_cycle_nodes.argtypes = [C.c_void_p, C.c_int]
         _lib.orc_neighbour_table.argtypes = [C.POINTER(_Grid), C.c_void_p, C.c_void_p]
         _lib.orc_set_threads.argtypes = [C.c_int]
+        _lib.orc_tree_accum_down_f32.argtypes = [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 3
+        _lib.orc_tree_max_down_f32.argtypes = [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 2
+        _lib.orc_erode_deposit_f32.argtypes = [C.c_void_p] * 5 + [C.c_float] * 7 + [C.c_void_p] * 2 + [C.c_int] + \
+            [C.c_void_p] * 3
         _lib.orc_ceil_log2.argtypes = [C.c_longlong]
     return _lib
 
@@ -304,3 +308,41 @@ def graphflood_run(zh, h, Q, g: Grid, dx, prec, manning=0.033, edgesw=1e-2, dt=5
     fn = lib().orc_graphflood_run_f64 if f64 else lib().orc_graphflood_run_f32
     fn(_p(zh), _p(h), _p(Q), g.ref, C.byref(prm), int(niter), _p(trace))
     return trace
+
+
+# ---- legacy downstream tree algorithms (archive/fastflow/kernels) ------------
+def tree_accum_down(rcv, W, p):
+    """tree_accum_down rounds; returns (rcv, W, p) as the reference leaves them."""
+    rcv = np.array(rcv, np.int32, copy=True)
+    W = np.array(W, np.float32, copy=True)
+    p = np.array(p, np.float32, copy=True)
+    N = p.size
+    r2, W2, p2 = np.empty_like(rcv), np.empty_like(W), np.empty_like(p)
+    lib().orc_tree_accum_down_f32(_p(rcv), _p(W), _p(p), N, _p(r2), _p(W2), _p(p2))
+    return rcv, W, p
+
+
+def tree_max_down(rcv, p):
+    """tree_max_down rounds; returns (rcv, p) as the reference leaves them."""
+    rcv = np.array(rcv, np.int32, copy=True)
+    p = np.array(p, np.float32, copy=True)
+    r2, p2 = np.empty_like(rcv), np.empty_like(p)
+    lib().orc_tree_max_down_f32(_p(rcv), _p(p), p.size, _p(r2), _p(p2))
+    return rcv, p
+
+
+def erode_deposit(z, bound, rcv, drain, Qs, dt, dx, k_spl, k_t, k_h, k_d, m):
+    """erode_deposit kernel + downstream solve; returns (z after deposition, new
+    elevations pe, We after the rounds)."""
+    z = np.array(z, np.float32, copy=True).ravel()
+    N = z.size
+    bound = np.ascontiguousarray(bound, np.uint8).ravel()
+    rcv = np.array(rcv, np.int32, copy=True).ravel()
+    drain = np.ascontiguousarray(drain, np.float32).ravel()
+    Qs = np.ascontiguousarray(Qs, np.float32).ravel()
+    pe, We = np.empty(N, np.float32), np.empty(N, np.float32)
+    r2, W2, p2 = np.empty(N, np.int32), np.empty(N, np.float32), np.empty(N, np.float32)
+    f = lambda x: float(np.float32(x))  # noqa: E731
+    lib().orc_erode_deposit_f32(_p(z), _p(bound), _p(rcv), _p(drain), _p(Qs), f(dt), f(dx), f(k_spl), f(k_t), f(k_h),
+                                f(k_d), f(m), _p(pe), _p(We), N, _p(r2), _p(W2), _p(p2))
+    return z, pe, We

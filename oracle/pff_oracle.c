@@ -538,3 +538,81 @@ typedef struct {
 #define SFX64(n) n##_f64
 GF_DRIVER(float, SFX32, int64_t)
 GF_DRIVER(double, SFX64, orc_key64)
+
+/* ---- legacy downstream tree algorithms (archive/fastflow/kernels) ---------
+ * Serial restatements; each round reads the start-of-round arrays (the
+ * reference double-buffers them and copies back after every round). */
+
+/* tree_accum_down.py:15-21, driven ceil(log2 n) times by
+ * _save_fasftflow/fastflow/tree_accum_down.py:20-34: p = p + W*p[rcv],
+ * W = W*W[rcv], rcv = rcv[rcv]; rcv, W and p end as the reference leaves them. */
+void orc_tree_accum_down_f32(int32_t *rcv, float *W, float *p, int N, int32_t *r2, float *W2, float *p2)
+{
+    const int rounds = orc_ceil_log2(N);
+    for (int it = 0; it < rounds; ++it) {
+        for (int i = 0; i < N; ++i) {
+            const int r = rcv[i];
+            const float t = W[i] * p[r];
+            p2[i] = p[i] + t;
+            W2[i] = W[i] * W[r];
+            r2[i] = rcv[r];
+        }
+        memcpy(rcv, r2, sizeof(int32_t) * (size_t)N);
+        memcpy(W, W2, sizeof(float) * (size_t)N);
+        memcpy(p, p2, sizeof(float) * (size_t)N);
+    }
+}
+
+/* tree_max_down.py:7-12 driven by _save_fasftflow/fastflow/tree_max_down.py:20-31:
+ * where rcv[rcv] != rcv, p = max(p[rcv], p) and rcv = rcv[rcv]; other nodes keep
+ * their values.  max(a, b) is taken as a > b ? a : b. */
+void orc_tree_max_down_f32(int32_t *rcv, float *p, int N, int32_t *r2, float *p2)
+{
+    const int rounds = orc_ceil_log2(N);
+    for (int it = 0; it < rounds; ++it) {
+        for (int i = 0; i < N; ++i) {
+            const int r = rcv[i];
+            if (rcv[r] != r) {
+                const float a = p[r], b = p[i];
+                p2[i] = a > b ? a : b;
+                r2[i] = rcv[r];
+            } else {
+                p2[i] = p[i];
+                r2[i] = r;
+            }
+        }
+        memcpy(rcv, r2, sizeof(int32_t) * (size_t)N);
+        memcpy(p, p2, sizeof(float) * (size_t)N);
+    }
+}
+
+/* erode_deposit.py:7-24 (deposition, implicit stream-power factors), then the
+ * downstream solve of _archived/erode_deposit.py:30-39: tree_accum_down on
+ * (rcv, We, pe).  z is updated by the deposition in place; pe ends as the new
+ * elevations (the reference's return value), We as its jumped weights; rcv is
+ * jumped in place.  Powers are taken in double and rounded once to f32. */
+void orc_erode_deposit_f32(float *z, const uint8_t *bound, int32_t *rcv, const float *drain, const float *Qs,
+                           float dt, float dx, float k_spl, float k_t, float k_h, float k_d, float m,
+                           float *pe, float *We, int N, int32_t *r2, float *W2, float *p2)
+{
+    for (int i = 0; i < N; ++i) {
+        if (!bound[i]) {
+            const float cd = fminf(k_d / drain[i], 1.0f);
+            const float dz = dt * cd;
+            z[i] += dz * Qs[i];
+        }
+        const float pm = (float)pow((double)drain[i], (double)m);
+        const float pmm = (float)pow((double)drain[i], (double)(-m));
+        float s = k_spl * pm;
+        s = s + k_t;
+        s = s + k_h * pmm;
+        const float K = (dt / dx) * s;
+        pe[i] = z[i] / (1.0f + K);
+        We[i] = K / (1.0f + K);
+        if (bound[i]) {
+            pe[i] = z[i];
+            We[i] = 0.0f;
+        }
+    }
+    orc_tree_accum_down_f32(rcv, We, pe, N, r2, W2, p2);
+}

@@ -10,5 +10,6 @@ __version__ = "0.1.0"
 from . import constants
 from . import flow
 from . import graphflood
+from . import archive
 
-__all__ = ["constants", "flow", "graphflood"]
+__all__ = ["constants", "flow", "graphflood", "archive"]

@@ -46,6 +46,10 @@ SIGNATURES = {
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
     "pff_abs_diff_stats": (_i32, [_vp, _vp, _i32, _vp, _vp]),
+    "pff_archive_workspace_bytes": (_sz, [_i32]),
+    "pff_tree_accum_down": (_i32, [_vp, _vp, _vp, _i32, _vp, _sz, _vp]),
+    "pff_tree_max_down": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp]),
+    "pff_erode_deposit": (_i32, [_vp] * 5 + [_f32] * 7 + [_vp, _vp, _i32, _vp, _sz, _vp]),
     "pff_batch_workspace_bytes": (_sz, [_i64, _i32]),
     "pff_batch_plan": (_i64, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
     "pff_batch_route": (_i32, [_vp] * 6 + [_i64, _i32, _i32, _i32, _vp, _sz, _vp]),

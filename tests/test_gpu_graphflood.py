@@ -115,3 +115,36 @@ def test_flooder_iterations(orc, cuda, mode):
     assert np.array_equal(bits(fl.get_h().ravel()), bits(h))
     assert np.array_equal(bits(router.get_Z().ravel()), bits(zh))
     assert np.array_equal(bits(router.get_Q().ravel()), bits(Q))
+
+
+@pytest.mark.gpu
+def test_graphflood_2048_50_iterations_match_oracle_fixture(cuda):
+    """The 2048 x 2048 GraphFlood benchmark DEM, 50 iterations through Flooder
+    (each with receivers, carve rerouting, fill, 5 diffusion sweeps, Manning):
+    h, zh and Q bit-identical to the CPU oracle's, compared through the SHA-256 of
+    their bit patterns recorded in tests/golden/graphflood_2048_50.json (written by
+    tests/golden/make_graphflood_2048_fixture.py)."""
+    import hashlib
+    import json
+    import os
+
+    import pyfastflow_b200 as pf
+
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "graphflood_2048_50.json")))
+    n = 2048
+    z = synthetic.graphflood_plain(n)["z"]
+    router = pf.flow.FlowRouter(n, n, 10.0)
+    router.set_z(z)
+    fl = pf.graphflood.Flooder(router, precipitation_rates=1e-5, manning=0.033, edge_slope=1e-2)
+    fl.run_graphflood(fx["iterations"])
+    cuda.cuda.synchronize()
+
+    def sha(a):
+        a = np.ascontiguousarray(a, np.float32).ravel()
+        b = a.view(np.uint32).copy()
+        b[np.isnan(a)] = 0x7FC00000
+        return hashlib.sha256(b.tobytes()).hexdigest()
+
+    assert sha(fl.get_h()) == fx["sha256"]["h"]
+    assert sha(router.get_Z()) == fx["sha256"]["zh"]
+    assert sha(router.get_Q()) == fx["sha256"]["Q"]

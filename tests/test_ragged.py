@@ -263,3 +263,27 @@ def test_ragged_custom_codes_bit_exact(orc, cuda):
         orc.graphflood_run(zh, h, Q, g, 10.0, 2e-5, manning=0.04, niter=25)
         assert np.array_equal(bits(fl.get_h(k)), bits(h)), f"tile {k} h"
         assert np.array_equal(bits(rr.Q[int(rr.offset[k]):int(rr.offset[k]) + rr.cells(k)].cpu().numpy()), bits(Q))
+
+
+@pytest.mark.gpu
+def test_ragged_config4_slice_bit_exact(orc, cuda):
+    """The first 48 tiles of the benchmark's ragged batch (512 tiles, sides
+    log-uniform in [128, 1024], 0-200 pits, normal / periodic east-west, seed 4)
+    routed in one launch, bit-exact per tile against the oracle."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+
+    tiles = synthetic.ragged_tiles(ntiles=48, seed=4)
+    sides = np.array([[t["nx"], t["ny"]] for t in tiles])
+    assert sides.min() >= 128 and sides.max() <= 1024 and len({t["mode"] for t in tiles}) == 2
+    rr = pf.flow.RaggedRouter([(t["ny"], t["nx"]) for t in tiles], 30.0, [t["mode"] for t in tiles])
+    rr.set_z([t["z"] for t in tiles])
+    rr.seed_constant(1.0, area=True)
+    rr.route(graph=True)
+    torch.cuda.synchronize()
+    seed = np.float32(900.0)
+    for k, t in enumerate(tiles):
+        _, r, Q, cnt = oracle_chain(orc, t, seed)
+        assert np.array_equal(rr.get_receivers(k).ravel(), r), f"tile {k} receivers"
+        assert np.array_equal(rr.get_counts(k).ravel(), cnt), f"tile {k} counts"
+        assert np.array_equal(bits(rr.get_Q(k)), bits(Q)), f"tile {k} Q"

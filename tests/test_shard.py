@@ -2,7 +2,8 @@
 (largest-first bin packing) and need no collective on the data path.  Checked here
 with 2 CPU ranks over gloo: the shares cover the batch exactly once, are balanced,
 and routing each share (with the oracle, the CPU stand-in for a rank's GPU) and
-gathering the results gives the single-process results."""
+gathering the whole per-tile arrays gives the single-process results.  A GPU test
+routes the same kind of shares through RaggedRouter, the product's sharded path."""
 import os
 import socket
 
@@ -49,8 +50,8 @@ def _rank_main(rank, world, port, out):
         g = orc.Grid(t["nx"], t["ny"], {"normal": 0, "periodic_EW": 1}[t["mode"]])
         rcv, _ = orc.compute_receivers(t["z"], g, t["dx"])
         r, _, _, _, _ = orc.reroute_flow(rcv, t["z"], g)
-        _, cnt = orc.accumulate(r, 1.0)
-        mine[k] = int(cnt.astype(np.int64).sum())
+        Q, cnt = orc.accumulate(r, 1.0)
+        mine[k] = (r, Q.view(np.uint32), cnt)  # whole per-tile arrays
     gathered = [None] * world
     dist.all_gather_object(gathered, (parts[rank], mine))  # results only; no data-path collective
     if rank == 0:
@@ -81,5 +82,41 @@ def test_two_gloo_ranks_cover_the_batch(orc):
         g = orc.Grid(t["nx"], t["ny"], {"normal": 0, "periodic_EW": 1}[t["mode"]])
         rcv, _ = orc.compute_receivers(t["z"], g, t["dx"])
         r, _, _, _, _ = orc.reroute_flow(rcv, t["z"], g)
-        _, cnt = orc.accumulate(r, 1.0)
-        assert results[k] == int(cnt.astype(np.int64).sum())
+        Q, cnt = orc.accumulate(r, 1.0)
+        rk, qk, ck = results[k]
+        assert np.array_equal(rk, r) and np.array_equal(qk, Q.view(np.uint32)) and np.array_equal(ck, cnt)
+
+
+@pytest.mark.gpu
+def test_sharded_shares_through_raggedrouter(orc, cuda):
+    """The product's sharded path on one GPU: each of two largest-first shares is
+    routed by its own RaggedRouter (what each rank runs), and every tile equals the
+    unsharded batch and the oracle, bit for bit."""
+    import pyfastflow_b200 as pf
+
+    tiles = synthetic.ragged_tiles(ntiles=10, seed=5, side_min=64, side_max=300, max_pits=40)
+    parts = partition_tiles([t["nx"] * t["ny"] for t in tiles], 2)
+    assert all(parts) and sorted(parts[0] + parts[1]) == list(range(10))
+
+    def route(sel):
+        rr = pf.flow.RaggedRouter([(tiles[k]["ny"], tiles[k]["nx"]) for k in sel], 30.0,
+                                  [tiles[k]["mode"] for k in sel])
+        rr.set_z([tiles[k]["z"] for k in sel])
+        rr.seed_constant(1.0, area=True)
+        rr.route(graph=True)
+        cuda.cuda.synchronize()
+        return {k: (rr.get_receivers(j).ravel(), rr.get_Q(j).ravel().view(np.uint32), rr.get_counts(j).ravel())
+                for j, k in enumerate(sel)}
+
+    whole = route(list(range(10)))
+    shards = {}
+    for p in parts:
+        shards.update(route(p))
+    for k, t in enumerate(tiles):
+        g = orc.Grid(t["nx"], t["ny"], {"normal": 0, "periodic_EW": 1}[t["mode"]])
+        rcv, _ = orc.compute_receivers(t["z"], g, t["dx"])
+        r, _, _, _, _ = orc.reroute_flow(rcv, t["z"], g)
+        Q, cnt = orc.accumulate(r, np.float32(900.0))
+        for got in (whole[k], shards[k]):
+            assert np.array_equal(got[0], r) and np.array_equal(got[1], Q.view(np.uint32))
+            assert np.array_equal(got[2], cnt)

@@ -258,3 +258,55 @@ def test_unet_training_reduces_loss(cuda):
         losses.append(float(loss))
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.6 * losses[0]
+
+
+@pytest.mark.gpu
+def test_warm_start_gain_over_cold_and_kinematic(cuda):
+    """What the trained network gains, on 16 held-out tiles (trained on 64 tiles of
+    64^2, 40 epochs: the benchmark's recipe at a scale a test can run):
+    - over the plain cold start: iterations until mean |dh|/dt < 1000 P drop by at
+      least half, and the mean residual 100 iterations in is at least 10x lower
+      (measured: 96 vs 2981 iterations, 984 P vs 56,875 P);
+    - over the same warm start without the network (the kinematic-wave depth, which
+      reaches residual thresholds faster still): the predicted depth is closer to the
+      plain solver's long-run depth (relative L1, measured 0.58 vs 0.92)."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+    from pyfastflow_b200.warmstart import UNet, make_dataset, scenario_tiles, train, warm_start_batch
+
+    side, niter = 64, 6000
+    x, tgt, wgt = make_dataset(64, side, niter, seed=10)
+    net = UNet(seed=0)
+    net.set_head_bias(float(tgt.mean()))
+    hist = train(net, x, tgt, side, weight=wgt, epochs=40, batch=16)
+    assert hist[-1] < hist[0]
+    etiles, eP, en = scenario_tiles(16, side, seed=99)
+    rr = pf.flow.RaggedRouter([t.shape for t in etiles], 10.0, "normal")
+    res, h0s = {}, {}
+    for arm in ("cold", "net", "kinematic"):
+        rr.set_z(etiles)
+        fl = pf.graphflood.RaggedFlooder(rr, precipitation_rates=eP, manning=en)
+        rr.Q.zero_()
+        extra = 0
+        if arm != "cold":
+            h0s[arm] = warm_start_batch(fl, net, arm).view(16, -1).clone()
+            extra = 1
+        _, _, tr = fl.run(niter - extra, stop=None, trace=True)
+        res[arm] = (tr[:, :, 1] / (5e-3 * eP[:, None]), extra)  # mean |dh| / dt over P, per iteration
+        if arm == "cold":
+            h_long = fl.h.view(16, -1).clone()  # the plain solver's state after niter iterations
+
+    def first_below(arm, tau):
+        r, extra = res[arm]
+        return np.median([int(np.argmax(r[k] < tau)) + 1 + extra if (r[k] < tau).any() else niter for k in range(16)])
+
+    assert first_below("net", 1000.0) <= 0.5 * first_below("cold", 1000.0)
+    at100 = {a: np.nanmedian(res[a][0][:, 100 - res[a][1]]) for a in res}
+    assert at100["net"] < 0.1 * at100["cold"], at100
+    ok = ~torch.isnan(h_long).any(1)
+    den = h_long.clamp_min(0).abs().sum(1)
+
+    def rel_l1(h0):
+        return ((h0 - h_long.clamp_min(0)).abs().sum(1) / den)[ok].cpu().numpy()
+
+    assert np.median(rel_l1(h0s["net"])) < np.median(rel_l1(h0s["kinematic"]))

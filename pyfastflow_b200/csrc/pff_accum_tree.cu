@@ -105,12 +105,36 @@ __device__ __forceinline__ int fixed_shift(unsigned maxbits, int N)
     const float m = __uint_as_float(maxbits);
     if (!(m > 0.f)) return 0;
     int e;
-    frexpf(m, &e);              // m < 2^e
-    int nb = 0;
-    while (nb < 31 && (1u << nb) <= (unsigned)N) ++nb;  // N < 2^nb
+    const unsigned E = (maxbits >> 23) & 0xffu;
+    if (E) e = (int)E - 126;    // m = f * 2^e with f in [0.5, 1): m < 2^e
+    else frexpf(m, &e);
+    const int nb = 32 - __clz(N);  // N < 2^nb
     return 62 - (e + nb);
 }
-__device__ __forceinline__ long long to_fixed(float w, int s) { return __double2ll_rn(scalbn((double)w, s)); }
+// round(w * 2^s) to the nearest integer, ties to even, from the IEEE-754 fields:
+// w = +-m * 2^(E-150) (m with its implicit bit; E = 0: m * 2^-149).  Exact in
+// 64 bits for every |w| <= max|seed| (fixed_shift keeps m * 2^(e+s) < 2^62).
+__device__ __forceinline__ long long to_fixed(float w, int s)
+{
+    const unsigned b = __float_as_uint(w);
+    const unsigned E = (b >> 23) & 0xffu;
+    unsigned long long m = b & 0x7fffffu;
+    int e;
+    if (E) { m |= 0x800000u; e = (int)E - 150; }
+    else e = -149;
+    const int sh = e + s;
+    unsigned long long v;
+    if (sh >= 0) v = sh < 40 ? m << sh : 0;  // (larger shifts only for non-finite seeds, flagged elsewhere)
+    else {
+        const int k = -sh;
+        if (k > 40) v = 0;
+        else {
+            const unsigned long long q = m >> k, rem = m & ((1ull << k) - 1), half = 1ull << (k - 1);
+            v = q + ((rem > half || (rem == half && (q & 1))) ? 1 : 0);
+        }
+    }
+    return (b >> 31) ? -(long long)v : (long long)v;
+}
 __device__ __forceinline__ float from_fixed(long long v, int s)
 {
     // one correct rounding to f32, then an exact power-of-two scaling
@@ -125,10 +149,21 @@ __global__ void k_tree_seedmax(const float *__restrict__ w, int N, int *status)
 {
     unsigned m = 0;
     bool bad = false;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const float a = fabsf(w[i]);
+    auto take = [&](float x) {
+        const float a = fabsf(x);
         if (!(a <= 3.4028235e38f)) bad = true;
         else m = max(m, __float_as_uint(a));
+    };
+    const int stride = gridDim.x * blockDim.x, t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (((uintptr_t)w & 15) == 0) {  // 16-byte loads, then the tail
+        const float4 *w4 = reinterpret_cast<const float4 *>(w);
+        for (int q = t0; q < N / 4; q += stride) {
+            const float4 v = __ldg(w4 + q);
+            take(v.x); take(v.y); take(v.z); take(v.w);
+        }
+        for (int i = (N / 4) * 4 + t0; i < N; i += stride) take(w[i]);
+    } else {
+        for (int i = t0; i < N; i += stride) take(w[i]);
     }
     for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0 && m) atomicMax((unsigned *)&status[1], m);
@@ -254,23 +289,26 @@ __global__ void __launch_bounds__(TR_T0_THREADS) k_tree_tile(const int32_t *__re
     __syncthreads();
     // doubling rounds: the longest in-tile path is < 1024 = 2^10 cells
     bool cyc = false;
+    unsigned alive = 0;  // this thread's cells whose pointer is still alive
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) alive |= (jmp[threadIdx.x + j * TR_T0_THREADS] >= 0 ? 1u : 0u) << j;
     for (int r = 0;; ++r) {
         int sj[RPT], nj[RPT];
         unsigned sl[RPT], sh[RPT], sc[RPT];
-        bool live = false;
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
             const int k = threadIdx.x + j * TR_T0_THREADS;
-            sj[j] = jmp[k];
-            if (sj[j] >= 0) {
+            sj[j] = -1;
+            if (alive >> j & 1u) {
+                sj[j] = jmp[k];
                 sl[j] = lo[k];
                 sh[j] = hi[k];
                 sc[j] = cnt[k];
                 nj[j] = jmp[sj[j]];
-                live = true;
+                if (nj[j] < 0) alive &= ~(1u << j);
             }
         }
-        if (!__syncthreads_or(live)) break;
+        if (!__syncthreads_or(sj[0] >= 0 || sj[1] >= 0 || sj[2] >= 0 || sj[3] >= 0)) break;
         if (r == 10) { cyc = true; break; }  // a path longer than the tile: a cycle
 #pragma unroll
         for (int j = 0; j < RPT; ++j) {
@@ -501,8 +539,12 @@ __global__ void __launch_bounds__(TR_LB_THREADS) k_tree_level(int L, TreeArgs a)
     for (int k = threadIdx.x; k < n; k += TR_LB_THREADS) tn[k] = lpar[k] >= 0 ? lpar[k] : k;
     __syncthreads();
     for (int r = 0; r <= rounds; ++r) {
-        for (int k = threadIdx.x; k < n; k += TR_LB_THREADS) tn[k] = tn[tn[k]];
-        __syncthreads();
+        bool ch = false;
+        for (int k = threadIdx.x; k < n; k += TR_LB_THREADS) {
+            const int t = tn[k], tt = tn[t];
+            if (tt != t) { tn[k] = tt; ch = true; }
+        }
+        if (!__syncthreads_or(ch)) break;
     }
     const TreeLevel &U = a.lv[L + 1];
     const int ubx = bx / 2, uby = by / 2;

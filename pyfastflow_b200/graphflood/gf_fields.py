@@ -10,7 +10,7 @@ from ..flow import fill_topo
 
 
 class Flooder:
-    def __init__(self, router, precipitation_rates=10e-3 / 3600, manning=0.033, edge_slope=1e-2):
+    def __init__(self, router, precipitation_rates=10e-3 / 3600, manning=0.033, edge_slope=1e-2, graphs=True):
         self.nx, self.ny, self.dx, self.rshp = router.nx, router.ny, router.dx, router.rshp
         self.router = router
         N = router.N
@@ -21,6 +21,8 @@ class Flooder:
         self.precipitation_rates = precipitation_rates
         self.manning = manning
         self.edge_slope = edge_slope
+        self.graphs = bool(graphs)  # replay the post-reroute part of an iteration from a CUDA graph
+        self._graphs = {}
         cte.PREC = precipitation_rates  # gf_fields.py:106-108
         cte.MANNING = manning
         cte.EDGESW = edge_slope
@@ -30,17 +32,13 @@ class Flooder:
         return dict(dx=f(self.dx), dx2=f(self.dx ** 2), prec_dx2=f(self.precipitation_rates * self.dx * self.dx),
                     manning=f(self.manning), edgesw=f(self.edge_slope), dt=f(cte.DT_HYDRO))
 
-    def iteration(self, track_dh: bool = False):
-        """One GraphFlood iteration (gf_fields.py:126-141): receivers, carve
-        reroute, fill with delta (epsilon 1e-3), 5 diffusion sweeps, Manning update."""
+    def _after_reroute(self, c, track_dh: bool):
+        """Fill with delta (epsilon 1e-3), 5 diffusion sweeps, Manning update."""
         r = self.router
-        c = self._consts()
         st = _dev.stream()
         if track_dh:
             self._h0.copy_(self.h)
             self._dhmax.zero_()
-        r.compute_receivers()
-        r.reroute_flow()
         fill_topo.fill_z_add_delta(r.z, self.h, r.z_, r.receivers, r.receivers_, r.receivers__, epsilon=1e-3,
                                    workspace=r._ws_fill)
         wp, wn = r._ws_diff.get(_lib.load().pff_diffuse_workspace_bytes(r.N), r.device)
@@ -50,6 +48,37 @@ class Flooder:
                   r.receivers.data_ptr(), r.Q.data_ptr(), r.N, c["dx"], c["dx2"], c["manning"], c["edgesw"],
                   c["dt"], self._h0.data_ptr() if track_dh else None, self._dhmax.data_ptr() if track_dh else None,
                   st)
+
+    def iteration(self, track_dh: bool = False):
+        """One GraphFlood iteration (gf_fields.py:126-141): receivers, carve
+        reroute, fill with delta (epsilon 1e-3), 5 diffusion sweeps, Manning update.
+        The part after the reroute (about 30 launches on fixed buffers) is replayed
+        from a CUDA graph captured on first use for these constants."""
+        r = self.router
+        c = self._consts()
+        r.compute_receivers()
+        r.reroute_flow()
+        if not self.graphs:
+            self._after_reroute(c, track_dh)
+            return
+        key = (track_dh,) + tuple(sorted(c.items()))
+        g = self._graphs.get(key)
+        if g is None:
+            # workspaces exist before the capture, so the graph only reads and writes them
+            r._ws_fill.get(_lib.load().pff_fill_workspace_bytes(r.N), r.device)
+            r._ws_diff.get(_lib.load().pff_diffuse_workspace_bytes(r.N), r.device)
+            g = torch.cuda.CUDAGraph()
+            torch.cuda.current_stream().synchronize()
+            try:
+                with torch.cuda.graph(g):
+                    self._after_reroute(c, track_dh)
+            except Exception:  # capture not possible here: stay eager
+                self.graphs = False
+                torch.cuda.synchronize()
+                self._after_reroute(c, track_dh)
+                return
+            self._graphs[key] = g
+        g.replay()
 
     def run_graphflood(self, N=10):
         """N iterations (gf_fields.py:111-141)."""

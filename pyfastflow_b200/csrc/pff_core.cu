@@ -168,6 +168,19 @@ __device__ __forceinline__ void rcv_pick1(float zi, const float (&zn)[4], const 
     if (!(dmax > 0.f)) return;
     const float q = __fdiv_rn(dmax, dx);
     if (!(q > 0.f)) return;
+    const unsigned qe = (__float_as_uint(q) >> 23) & 0xffu;
+    if (qe == 0u || qe == 255u) {
+        // subnormal or infinite quotients: drops far apart can round to the same
+        // value, so take the reference's ordered scan with a strict '>' (:43-52)
+        float best = 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (jn[k] == -1) continue;
+            const float t = __fdiv_rn(d[k], dx);
+            if (t > best) { best = t; r = jn[k]; sr = t; }
+        }
+        return;
+    }
     const float near = __fmul_rn(dmax, 1.0f - 0x1p-21f);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -194,6 +207,22 @@ __device__ __forceinline__ void rcv_pick_interior(float zi, float zt, float zl, 
     if (!(dmax > 0.f)) return;
     const float q = __fdiv_rn(dmax, dx);
     if (!(q > 0.f)) return;
+    const unsigned qe = (__float_as_uint(q) >> 23) & 0xffu;
+    if (qe == 0u || qe == 255u) {
+        // subnormal or infinite quotients: drops far apart can round to the same
+        // value, so take the reference's ordered scan with a strict '>' (:43-52)
+        const float dk[4] = {d0, d1, d2, d3};
+        const int off[4] = {-nx, -1, 1, nx};
+        float best = 0.f;
+        int kk = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float t = __fdiv_rn(dk[k], dx);
+            if (t > best) { best = t; kk = k; }
+        }
+        if (kk >= 0) { r = i + off[kk]; sr = best; }
+        return;
+    }
     // the first direction reaching q: an exact maximum, unless an earlier drop ties after
     // rounding (only possible within a few ulps of dmax: the rare slow path below)
     const float near = __fmul_rn(dmax, 1.0f - 0x1p-21f);

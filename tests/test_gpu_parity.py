@@ -357,3 +357,27 @@ def test_routing_lakes_4096_bit_exact(orc, cuda):
     assert np.array_equal(router.get_counts().ravel(), co)
     assert np.array_equal(router.get_Q().ravel().view(np.uint32), Qo.view(np.uint32))
     assert orc.count_cycle_nodes(r2) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dx", [0.3, 1.0, 7.3, 29.999, 1e-3, 1e4, 3.0e-20])
+def test_receivers_division_any_dx(orc, cuda, dx):
+    """The receivers kernel divides by dx with a reciprocal and an exact residual
+    check (IEEE division only where the check cannot decide): receivers and
+    gradients must equal the oracle's IEEE quotients for any dx, on drops from
+    tiny (subnormal quotients) to huge."""
+    torch = cuda
+    from pyfastflow_b200 import flow
+
+    rng = np.random.default_rng(int(dx * 1000) % 97)
+    nx, ny = 256, 96
+    z = (rng.random((ny, nx)) * 10.0 ** rng.integers(-30, 30, (ny, nx))).astype(np.float32)
+    z[:8] = rng.integers(0, 5, (8, nx)).astype(np.float32)  # exact ties
+    g = Grid(orc, torch, nx, ny, 0)
+    set_constants(g, dx)
+    rcv, grad = orc.compute_receivers(z, g.og, dx)
+    r = torch.empty(g.N, dtype=torch.int32, device="cuda")
+    gr = torch.empty(g.N, dtype=torch.float32, device="cuda")
+    flow.compute_receivers(dev(torch, z.ravel()), r, gr)
+    assert np.array_equal(host(r), rcv)
+    assert np.array_equal(fbits(host(gr)), fbits(grad))

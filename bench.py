@@ -12,8 +12,12 @@ DEM and weights copied from pinned host memory and Q + counts copied back, every
 step, inside the timed region.
 
 --impl reference times the CPU restatement of the reference algorithm (the
-reference itself is Python on Taichi, which is not installable here) on a
-bounded sample of the same workload with all host threads.
+reference itself is Python on Taichi, which is not installable here) on the
+same full workload with all host threads, one chain per step.
+
+roofline: the kernel with the largest event time per step among the probed
+kernels (library-side CUDA events around each launch, in a separate pass with
+the reroute loop driven from the host so that its kernels launch one by one).
 """
 from __future__ import annotations
 
@@ -36,6 +40,16 @@ METRIC = "Mcells/s route+reroute+accumulate"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # algorithmic bytes per cell (z in, rcv+gradient out | rcv+z in, rcv+bid out | rcv+w in, Q+counts out)
 ALG_BYTES = {"receivers": 12, "reroute": 16, "accumulate": 16}
+# Probed kernels: algorithmic bytes per cell of a launch over the whole grid
+# (None: the launch covers a varying list of tiles), and DRAM read + write bytes
+# of one 4096^2 launch from an ncu capture of this workload (None: not captured).
+KERNELS = {
+    "k_receivers": (12, 146.0e6),           # z in; receivers + gradient out
+    "k_tile_terminal<grid>": (8, None),     # receivers in; tile terminals out
+    "k_tile_terminal<list>": (None, None),  # the tiles a carve changed
+    "k_tree_tile<up>": (8, 251.0e6),        # receivers + seeds in
+    "k_tree_tile<down>": (16, 323.0e6),     # receivers + seeds in; Q + counts out
+}
 
 
 def peak_hbm():
@@ -309,19 +323,50 @@ def main():
         for k, name in enumerate(stages):
             stages[name].append(e[k].elapsed_time(e[k + 1]))
     st_ms = {k: sum(v) / len(v) for k, v in stages.items()}
-    dom = max(st_ms, key=st_ms.get)
     pk, pk_kind = peak_hbm()
-    ach = ALG_BYTES[dom] * n * n / (st_ms[dom] * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk, "unit": "GB/s", "frac": ach / pk,
-                "peak_source": pk_kind, "traffic": None,
-                "alg_bytes_per_cell": ALG_BYTES[dom], "stage_ms": st_ms}
-    # the stencil stage (one kernel: receivers), 12 algorithmic bytes per cell
-    ach_s = ALG_BYTES["receivers"] * n * n / (st_ms["receivers"] * 1e-3) / 1e9
-    roofline_stencil = {"bound": "hbm", "kernel": "receivers", "achieved": ach_s, "peak": pk, "unit": "GB/s",
-                        "frac": ach_s / pk, "peak_source": pk_kind, "alg_bytes_per_cell": ALG_BYTES["receivers"],
-                        "traffic": 146e6 * (n * n) / 16777216.0,
-                        "traffic_note": "DRAM read+write of one 4096^2 launch from an ncu capture (67 + 79 MB), "
-                                        "scaled by cells"}
+
+    # ---- per-kernel event times (separate pass, probes armed) -> roofline ----
+    import ctypes
+
+    prev_graphs = lib.pff_reroute_use_graphs(0)
+    lib.pff_probe_enable(1)
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        step()
+    torch.cuda.synchronize()
+    kernels = {}
+    for name, (bpc, traffic) in KERNELS.items():
+        tot, nl = ctypes.c_double(), ctypes.c_int()
+        if lib.pff_probe_read(name.encode(), ctypes.byref(tot), ctypes.byref(nl)) != 0 or nl.value == 0:
+            continue
+        per = tot.value / nl.value
+        k = {"ms_per_launch": per, "launches_per_step": nl.value / args.steps, "ms_per_step": tot.value / args.steps}
+        if bpc is not None:
+            k["alg_bytes_per_launch"] = bpc * n * n
+            k["achieved_gbs"] = bpc * n * n / (per * 1e-3) / 1e9
+            k["frac"] = k["achieved_gbs"] / pk
+            k["traffic"] = traffic * (n * n) / 16777216.0 if traffic else None
+        kernels[name] = k
+    lib.pff_probe_enable(0)
+    lib.pff_reroute_use_graphs(prev_graphs)
+    timed = [k for k in kernels if "alg_bytes_per_launch" in kernels[k]]
+    dom = max(timed, key=lambda k: kernels[k]["ms_per_step"])
+    kd = kernels[dom]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": kd["achieved_gbs"], "peak": pk, "unit": "GB/s",
+                "frac": kd["frac"], "peak_source": pk_kind, "traffic": kd["traffic"],
+                "alg_bytes_per_launch": kd["alg_bytes_per_launch"], "ms_per_launch": kd["ms_per_launch"],
+                "traffic_note": "DRAM read + write of one launch of this workload from an ncu capture",
+                "kernels": kernels, "stage_ms": st_ms}
+    # the stencil kernel (receivers), 12 algorithmic bytes per cell
+    kr = kernels.get("k_receivers")
+    roofline_stencil = None
+    if kr:
+        roofline_stencil = {"bound": "hbm", "kernel": "k_receivers", "achieved": kr["achieved_gbs"], "peak": pk,
+                            "unit": "GB/s", "frac": kr["frac"], "peak_source": pk_kind,
+                            "alg_bytes_per_launch": kr["alg_bytes_per_launch"], "ms_per_launch": kr["ms_per_launch"],
+                            "traffic": kr["traffic"],
+                            "traffic_note": "DRAM read+write of one 4096^2 launch from an ncu capture (67 + 79 MB), "
+                                            "scaled by cells"}
 
     # ---- e2e through the public API with host buffers ----
     zh = torch.from_numpy(z.ravel()).pin_memory()

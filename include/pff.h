@@ -45,6 +45,21 @@ const char *pff_last_error_string(void);
 /* Total number of CUDA kernels this library has launched in this process (no
  * counterpart in the reference: used to report GPU launches per step). */
 long long pff_launch_count(void);
+/* Kernel timing probes (no reference counterpart; used by benchmarks to time the
+ * dominant kernels inside a call).  pff_probe_enable(1) clears and arms them: each
+ * probed launch made outside stream capture is then bracketed by two CUDA events on
+ * its own stream (at most 512 launches per kernel name).  pff_probe_enable(0)
+ * disarms and clears.  pff_probe_read waits for the recorded events of the kernel
+ * named `name` (for example "k_tree_tile<up>") and returns their summed event time
+ * in milliseconds and the number of probed launches (0 if it never ran). */
+int pff_probe_enable(int on);
+int pff_probe_read(const char *name, double *total_ms, int *launches);
+/* Whether pff_reroute_flow drives its outer loop from a device-side CUDA graph
+ * (1, the default) or from the host (0: one synchronisation per outer iteration;
+ * its kernels can then be profiled and probed one by one).  The environment
+ * variable PFF_REROUTE_NO_GRAPH makes 0 the default.  Returns the previous
+ * setting.  No reference counterpart. */
+int pff_reroute_use_graphs(int on);
 /* Make `device` current for this library's calls on the calling host thread
  * (the library links its own CUDA runtime; callers that use several GPUs set
  * the device that owns the buffers before calling).  No reference counterpart. */

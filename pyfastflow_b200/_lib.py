@@ -20,6 +20,9 @@ SIGNATURES = {
     "pff_version": (_i32, []),
     "pff_last_error_string": (C.c_char_p, []),
     "pff_launch_count": (C.c_longlong, []),
+    "pff_probe_enable": (_i32, [_i32]),
+    "pff_probe_read": (_i32, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "pff_reroute_use_graphs": (_i32, [_i32]),
     "pff_set_device": (_i32, [_i32]),
     "pff_compute_receivers": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, _vp]),
     "pff_compute_receivers_stochastic": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, C.c_uint64, _vp]),

@@ -703,7 +703,9 @@ extern "C" int pff_accumulate_tree(const int32_t *receivers, const float *weight
     PFF_CUDA(cudaFuncSetAttribute(k_tree_level<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     PFF_CUDA(cudaFuncSetAttribute(k_tree_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     PFF_CUDA(cudaFuncSetAttribute(k_tree_level<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    { k_tree_tile<false><<<p.ntiles, TR_T0_THREADS, 0, st>>>(receivers, weights, value, Q, counts, a); count_launch(); }
+    PFF_PROBED("k_tree_tile<up>", st,
+               k_tree_tile<false><<<p.ntiles, TR_T0_THREADS, 0, st>>>(receivers, weights, value, Q, counts, a));
+    count_launch();
     for (int L = 1; L < p.nlev; ++L) {
         k_tree_level<0><<<p.nb[L], TR_LB_THREADS, smem, st>>>(L, a);
         count_launch();
@@ -713,7 +715,9 @@ extern "C" int pff_accumulate_tree(const int32_t *receivers, const float *weight
         k_tree_level<1><<<p.nb[L], TR_LB_THREADS, smem, st>>>(L, a);
         count_launch();
     }
-    { k_tree_tile<true><<<p.ntiles, TR_T0_THREADS, 0, st>>>(receivers, weights, value, Q, counts, a); count_launch(); }
+    PFF_PROBED("k_tree_tile<down>", st,
+               k_tree_tile<true><<<p.ntiles, TR_T0_THREADS, 0, st>>>(receivers, weights, value, Q, counts, a));
+    count_launch();
     return check_cuda("pff_accumulate_tree");
 }
 

@@ -5,6 +5,7 @@
 // the library is built with -fmad=false), so each operation is the reference's
 // single IEEE operation in the reference's order.
 #include <algorithm>
+#include <cstdlib>
 #include "pff_internal.h"
 
 namespace pff {
@@ -22,6 +23,57 @@ __global__ void __launch_bounds__(256) k_fill_round(const float *__restrict__ zh
     const float zi = zs[i];
     if (i == r || (zi > zh[r] && rr == r)) { zn[i] = zi; return; }  // :32
     zn[i] = fmaxf(zi, __fadd_rn(zs[r], inc));              // :36
+}
+
+// The same rounds on one 8-byte record per cell, {pointer, snapshot z}: a round reads
+// its own record and gathers the record at its pointer (one sector instead of three
+// gathers), then writes its new record.  zh[r] is needed only where r points to
+// itself; at a cell whose receiver is itself from the start, the snapshot never
+// changes (:32 keeps it), so zs[r] is zh[r] there.  Bit 31 of the pointer word marks
+// those cells; a self-pointer made by a receiver cycle (no such bit) reads zh[r].
+constexpr uint32_t FILL_ROOT = 0x80000000u;
+__global__ void __launch_bounds__(256) k_fill_pack(const float *__restrict__ zh, const int32_t *__restrict__ rcv,
+                                                   uint2 *__restrict__ A, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int r = rcv[i];
+    A[i] = make_uint2((uint32_t)r | (r == i ? FILL_ROOT : 0u), __float_as_uint(zh[i]));
+}
+
+__global__ void __launch_bounds__(256) k_fill_round_packed(const float *__restrict__ zh, const uint2 *__restrict__ A,
+                                                           uint2 *__restrict__ B, float inc, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const uint2 me = A[i];
+    const int r = (int)(me.x & ~FILL_ROOT);
+    const uint2 at = A[r];
+    const int rr = (int)(at.x & ~FILL_ROOT);
+    const float zi = __uint_as_float(me.y), zr = __uint_as_float(at.y);
+    B[i].x = (uint32_t)rr | (me.x & FILL_ROOT);           // :29
+    float zn;
+    if (i == r) zn = zi;
+    else if (rr == r && zi > ((at.x & FILL_ROOT) ? zr : zh[r])) zn = zi;  // :32
+    else zn = fmaxf(zi, __fadd_rn(zr, inc));              // :36
+    B[i].y = __float_as_uint(zn);
+}
+
+// the packed result to z_ and both receiver buffers (:39-40), then, if h is given,
+// _apply_fill_z_add_delta (:82-97); write_z copies z_ into zh without a depth update
+__global__ void __launch_bounds__(256) k_fill_unpack(const uint2 *__restrict__ A, float *z_, int32_t *r1, int32_t *r2,
+                                                     float *zh, float *h, bool write_z, int N)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const uint2 a = A[i];
+    const int r = (int)(a.x & ~FILL_ROOT);
+    const float zf = __uint_as_float(a.y);
+    z_[i] = zf;
+    r1[i] = r;
+    r2[i] = r;
+    if (h) h[i] = __fadd_rn(h[i], __fsub_rn(zf, zh[i]));
+    if (h || write_z) zh[i] = zf;
 }
 
 // _apply_fill_z_add_delta (:82-97)
@@ -101,6 +153,176 @@ __global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__
             if (neighbour_i<MODE>(g, i, k) == j) acc = __fadd_rn(acc, __fmul_rn(w[k * N + i], qi));
     }
     Qn[j] = acc;
+}
+
+// ---- diffusion, all sweeps in one pass (boundary modes 0-2) -----------------------
+// A 64 x 16 tile with a halo of H = nsweeps cells: sweep s is valid on the region
+// shrunk by s, so after H sweeps the tile itself is exact.  Per block: zh over the
+// region and one more ring (the weights of the region's cells need their
+// neighbours), then each region cell's four outgoing weights and source flag
+// computed with the weight kernel's operations, then the sweeps on a shrinking
+// band, double-buffered in shared memory.  Traffic: zh and Q over the region once,
+// temp once.
+//
+// Periodic modes load the halo with wrap-around, so in modes 0-2 (nx, ny >= 3) the
+// k-th neighbour of a cell is always the adjacent shared-memory cell, and it exists
+// exactly when that cell lies in the grid along the non-periodic axes.  A cell that
+// cannot leave the domain has all four neighbours.  The sources of a cell are
+// gathered in ascending global index (the serial order of the reference's atomics):
+// top, left, right, bottom, except at the wrapped edges -- periodic EW columns 0 and
+// nx-1: top, right, left, bottom; periodic NS row 0: left, right, bottom, top; row
+// ny-1: bottom, top, left, right.  Flag byte per region cell: bit 0 in the grid,
+// bit 1 a source, bits 2-3 that order.
+constexpr int DF_TX = 64, DF_TY = 16, DF_HMAX = 8;
+__host__ __device__ constexpr int df_region(int H) { return (DF_TX + 2 * H) * (DF_TY + 2 * H); }
+__host__ __device__ constexpr int df_ring(int H) { return (DF_TX + 2 * H + 2) * (DF_TY + 2 * H + 2); }
+// zh over the region and its ring, four weight planes, two Q buffers, the flags
+constexpr size_t df_smem(int H) { return sizeof(float) * (size_t)(df_ring(H) + 6 * df_region(H)) + df_region(H); }
+
+template <int MODE>
+__device__ __forceinline__ bool df_inside(const Grid &g, int r, int c)
+{
+    return (MODE == 2 || (r >= 0 && r < g.ny)) && (MODE == 1 || (c >= 0 && c < g.nx));
+}
+__device__ __forceinline__ int df_wrap(int v, int n) { return (v >= 0 && v < n) ? v : ((v % n) + n) % n; }
+
+__device__ __forceinline__ float df_add(float acc, unsigned char f, float w, float q)
+{
+    return (f & 2) ? __fadd_rn(acc, __fmul_rn(w, q)) : acc;
+}
+
+template <int MODE, int H>
+__global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__ zh, const float *__restrict__ Qin,
+                                                       float *__restrict__ out, Grid g, float dx, float prec_dx2)
+{
+    constexpr int RX = DF_TX + 2 * H, RY = DF_TY + 2 * H, ZX = RX + 2, ZY = RY + 2, P = RX * RY;
+    extern __shared__ __align__(16) float df_sm[];
+    float *zs = df_sm;
+    float *w0 = zs + ZX * ZY, *w1 = w0 + P, *w2 = w1 + P, *w3 = w2 + P;
+    float *qa = w3 + P, *qb = qa + P;
+    unsigned char *fl = reinterpret_cast<unsigned char *>(qb + P);
+    const int x0 = blockIdx.x * DF_TX - H, y0 = blockIdx.y * DF_TY - H;  // region origin (unwrapped)
+    for (int t = threadIdx.x; t < ZX * ZY; t += blockDim.x) {
+        const int r = y0 - 1 + t / ZX, c = x0 - 1 + t % ZX;
+        zs[t] = df_inside<MODE>(g, r, c) ? zh[df_wrap(r, g.ny) * g.nx + df_wrap(c, g.nx)] : 0.f;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+        const int ry = t / RX, rx = t % RX, r = y0 + ry, c = x0 + rx;
+        unsigned char f = 0;
+        float q = 0.f, wk[4] = {0.f, 0.f, 0.f, 0.f};
+        if (df_inside<MODE>(g, r, c)) {
+            const int row = df_wrap(r, g.ny), col = df_wrap(c, g.nx);
+            q = Qin[row * g.nx + col];
+            f = 1;
+            const bool redge = row == 0 || row == g.ny - 1, cedge = col == 0 || col == g.nx - 1;
+            if (MODE == 1 && cedge) f |= 1 << 2;
+            if (MODE == 2 && redge) f |= (row == 0 ? 2 : 3) << 2;
+            const bool leave = MODE == 0 ? (redge || cedge) : (MODE == 1 ? redge : cedge);
+            if (!leave) {  // all four neighbours exist
+                const int z = (ry + 1) * ZX + rx + 1;
+                const float zi = zs[z];
+                const float zn[4] = {zs[z - ZX], zs[z - 1], zs[z + 1], zs[z + ZX]};
+                float sk[4], sums = 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    sk[k] = fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zn[k]), dx));
+                    sums = __fadd_rn(sums, sk[k]);
+                }
+                if (sums != 0.f) {
+                    f |= 2;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) wk[k] = __fdiv_rn(sk[k], sums);
+                }
+            }
+        }
+        w0[t] = wk[0];
+        w1[t] = wk[1];
+        w2[t] = wk[2];
+        w3[t] = wk[3];
+        qa[t] = q;
+        fl[t] = f;
+    }
+    __syncthreads();
+    float *qc = qa, *qn = qb;
+#pragma unroll
+    for (int sw = 1; sw <= H; ++sw) {
+        const int bw = RX - 2 * sw, bh = RY - 2 * sw;
+        for (int t = threadIdx.x; t < bw * bh; t += blockDim.x) {
+            const int i = (sw + t / bw) * RX + sw + t % bw;
+            const unsigned char f = fl[i];
+            if (!(f & 1)) continue;
+            // the source above reaches i through its bottom link (w3), the left one
+            // through its right link (w2), the right one its left (w1), below its top (w0)
+            const int u = i - RX, l = i - 1, rt = i + 1, d = i + RX;
+            float acc = prec_dx2;
+            switch (f >> 2) {
+            case 0:
+                acc = df_add(acc, fl[u], w3[u], qc[u]);
+                acc = df_add(acc, fl[l], w2[l], qc[l]);
+                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
+                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                break;
+            case 1:
+                acc = df_add(acc, fl[u], w3[u], qc[u]);
+                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
+                acc = df_add(acc, fl[l], w2[l], qc[l]);
+                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                break;
+            case 2:
+                acc = df_add(acc, fl[l], w2[l], qc[l]);
+                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
+                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                acc = df_add(acc, fl[u], w3[u], qc[u]);
+                break;
+            default:
+                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                acc = df_add(acc, fl[u], w3[u], qc[u]);
+                acc = df_add(acc, fl[l], w2[l], qc[l]);
+                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
+                break;
+            }
+            qn[i] = acc;
+        }
+        __syncthreads();
+        float *tq = qc;
+        qc = qn;
+        qn = tq;
+    }
+    for (int t = threadIdx.x; t < DF_TX * DF_TY; t += blockDim.x) {
+        const int ly = t / DF_TX, lx = t % DF_TX;
+        const int row = y0 + H + ly, col = x0 + H + lx;
+        if (row < g.ny && col < g.nx) out[row * g.nx + col] = qc[(H + ly) * RX + H + lx];
+    }
+}
+
+template <int MODE, int H>
+static int l_diffuse_fused_h(const float *zh, float *Q, float *temp, const Grid &g, float dx, float prec_dx2,
+                             cudaStream_t st)
+{
+    PFF_CUDA(cudaFuncSetAttribute(k_diffuse_fused<MODE, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)df_smem(H)));
+    dim3 gr(div_up(g.nx, DF_TX), div_up(g.ny, DF_TY));
+    PFF_PROBED("k_diffuse_fused", st,
+               k_diffuse_fused<MODE, H><<<gr, 256, df_smem(H), st>>>(zh, Q, temp, g, dx, prec_dx2));
+    count_launch();
+    return PFF_OK;
+}
+
+template <int MODE>
+static int l_diffuse_fused(const float *zh, float *Q, float *temp, int nsweeps, const Grid &g, float dx,
+                           float prec_dx2, cudaStream_t st)
+{
+    switch (nsweeps) {
+    case 1: return l_diffuse_fused_h<MODE, 1>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 2: return l_diffuse_fused_h<MODE, 2>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 3: return l_diffuse_fused_h<MODE, 3>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 4: return l_diffuse_fused_h<MODE, 4>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 5: return l_diffuse_fused_h<MODE, 5>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 6: return l_diffuse_fused_h<MODE, 6>(zh, Q, temp, g, dx, prec_dx2, st);
+    case 7: return l_diffuse_fused_h<MODE, 7>(zh, Q, temp, g, dx, prec_dx2, st);
+    default: return l_diffuse_fused_h<MODE, 8>(zh, Q, temp, g, dx, prec_dx2, st);
+    }
 }
 
 // ---- Manning update (gf_hydrodynamics.py:79-129) ------------------------------
@@ -194,7 +416,32 @@ static void l_diffuse(const float *zh, float *Q, float *temp, float *w, uint8_t 
 
 using namespace pff;
 
-extern "C" size_t pff_fill_workspace_bytes(int N) { return Carver::round(sizeof(float) * (size_t)N) + 256; }
+static bool g_diffuse_unfused = getenv("PFF_DIFFUSE_UNFUSED") != nullptr;  // diagnostics: the per-sweep kernels
+
+extern "C" size_t pff_fill_workspace_bytes(int N)
+{
+    if (N < 1) return 256;
+    return 2 * Carver::round(sizeof(uint2) * (size_t)N) + 256;
+}
+
+// ceil(log2 N) rounds (:121) of the packed fill; `inc(it)` is round it's increment.
+// Returns the buffer holding the last round's records.
+template <class Inc>
+static uint2 *fill_rounds(const float *zh, const int32_t *receivers, void *workspace, size_t workspace_bytes, int N,
+                          Inc inc, cudaStream_t st)
+{
+    Carver cv(workspace, workspace_bytes);
+    uint2 *a = cv.take<uint2>(N), *b = cv.take<uint2>(N);
+    { k_fill_pack<<<div_up(N, 256), 256, 0, st>>>(zh, receivers, a, N); count_launch(); }  // :116-117
+    int nr = 0;
+    for (long long p = 1; p < N; p <<= 1) ++nr;
+    for (int it = 0; it < nr; ++it) {
+        PFF_PROBED("k_fill_round_packed", st, k_fill_round_packed<<<div_up(N, 256), 256, 0, st>>>(zh, a, b, inc(it), N));
+        count_launch();
+        std::swap(a, b);
+    }
+    return a;
+}
 
 extern "C" int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_t *receivers, int32_t *receivers_,
                                     int32_t *receivers__, double epsilon, int N, void *workspace,
@@ -210,25 +457,10 @@ extern "C" int pff_fill_z_add_delta(float *zh, float *h, float *z_, const int32_
         return PFF_ERR_WORKSPACE;
     }
     cudaStream_t st = S(stream);
-    Carver cv(workspace, workspace_bytes);
-    float *zt = cv.take<float>(N);
-    const size_t nbf = sizeof(float) * (size_t)N, nbi = sizeof(int32_t) * (size_t)N;
-    PFF_CUDA(cudaMemcpyAsync(z_, zh, nbf, cudaMemcpyDeviceToDevice, st));              // :116
-    PFF_CUDA(cudaMemcpyAsync(receivers_, receivers, nbi, cudaMemcpyDeviceToDevice, st));  // :117
-    int nr = 0;
-    for (long long p = 1; p < N; p <<= 1) ++nr;  // ceil(log2 N), :121
-    float *zs = z_, *zn = zt;
-    int32_t *ra = receivers_, *rb = receivers__;
-    for (int it = 0; it < nr; ++it) {
-        const float inc = (float)(ldexp(1.0, it - 1) * epsilon);  // Python folds 2**(it-1)*eps in double
-        { k_fill_round<<<div_up(N, 256), 256, 0, st>>>(zh, zs, zn, ra, rb, inc, N); count_launch(); }
-        float *tz = zs; zs = zn; zn = tz;
-        int32_t *tr = ra; ra = rb; rb = tr;
-    }
-    if (zs != z_) PFF_CUDA(cudaMemcpyAsync(z_, zs, nbf, cudaMemcpyDeviceToDevice, st));
-    // both receiver buffers end with the final jumped pointers (:39-40)
-    PFF_CUDA(cudaMemcpyAsync(rb, ra, nbi, cudaMemcpyDeviceToDevice, st));
-    { k_fill_apply<<<div_up(N, 256), 256, 0, st>>>(zh, h, z_, N); count_launch(); }
+    // Python folds 2**(it-1)*eps in double
+    const uint2 *a = fill_rounds(zh, receivers, workspace, workspace_bytes, N,
+                                 [&](int it) { return (float)(ldexp(1.0, it - 1) * epsilon); }, st);
+    { k_fill_unpack<<<div_up(N, 256), 256, 0, st>>>(a, z_, receivers_, receivers__, zh, h, false, N); count_launch(); }
     return check_cuda("pff_fill_z_add_delta");
 }
 
@@ -325,24 +557,11 @@ extern "C" int pff_topofill(float *z, float *z_, const int32_t *receivers, int32
         return PFF_ERR_WORKSPACE;
     }
     cudaStream_t st = S(stream);
-    Carver cv(workspace, workspace_bytes);
-    float *zt = cv.take<float>(N);
-    const size_t nbf = sizeof(float) * (size_t)N, nbi = sizeof(int32_t) * (size_t)N;
-    PFF_CUDA(cudaMemcpyAsync(z_, z, nbf, cudaMemcpyDeviceToDevice, st));
-    PFF_CUDA(cudaMemcpyAsync(receivers_, receivers, nbi, cudaMemcpyDeviceToDevice, st));
-    int nr = 0;
-    for (long long p = 1; p < N; p <<= 1) ++nr;
-    float *zs = z_, *zn = zt;
-    int32_t *ra = receivers_, *rb = receivers__;
-    for (int it = 0; it < nr; ++it) {
-        const float inc = (float)(ldexp(1.0, it) * epsilon);  // = 2^it * float(epsilon): a power-of-2 scaling
-        { k_fill_round<<<div_up(N, 256), 256, 0, st>>>(z, zs, zn, ra, rb, inc, N); count_launch(); }
-        float *tz = zs; zs = zn; zn = tz;
-        int32_t *tr = ra; ra = rb; rb = tr;
-    }
-    if (zs != z_) PFF_CUDA(cudaMemcpyAsync(z_, zs, nbf, cudaMemcpyDeviceToDevice, st));
-    PFF_CUDA(cudaMemcpyAsync(rb, ra, nbi, cudaMemcpyDeviceToDevice, st));
-    if (write_back) PFF_CUDA(cudaMemcpyAsync(z, z_, nbf, cudaMemcpyDeviceToDevice, st));
+    // 2^it * float(epsilon): a power-of-2 scaling
+    const uint2 *a = fill_rounds(z, receivers, workspace, workspace_bytes, N,
+                                 [&](int it) { return (float)(ldexp(1.0, it) * epsilon); }, st);
+    { k_fill_unpack<<<div_up(N, 256), 256, 0, st>>>(a, z_, receivers_, receivers__, z, nullptr, write_back != 0, N);
+      count_launch(); }
     return check_cuda("pff_topofill");
 }
 
@@ -366,6 +585,18 @@ extern "C" int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps
     if (nsweeps == 0) return PFF_OK;
     Grid g{nx, ny, bound_mode, codes};
     cudaStream_t st = S(stream);
+    if (bound_mode != 3 && nx >= 3 && ny >= 3 && nsweeps <= DF_HMAX && !g_diffuse_unfused) {
+        // every sweep in one pass into temp (Q is read as other tiles' halo), then Q = temp (:74-75)
+        int rc = PFF_OK;
+        switch (bound_mode) {
+        case 0: rc = l_diffuse_fused<0>(zh, Q, temp, nsweeps, g, dx, prec_dx2, st); break;
+        case 1: rc = l_diffuse_fused<1>(zh, Q, temp, nsweeps, g, dx, prec_dx2, st); break;
+        default: rc = l_diffuse_fused<2>(zh, Q, temp, nsweeps, g, dx, prec_dx2, st); break;
+        }
+        PFF_TRY(rc);
+        PFF_CUDA(cudaMemcpyAsync(Q, temp, sizeof(float) * (size_t)N, cudaMemcpyDeviceToDevice, st));
+        return check_cuda("pff_diffuse_q");
+    }
     Carver cv(workspace, workspace_bytes);
     float *w = cv.take<float>(4 * (size_t)N);
     uint8_t *issrc = cv.take<uint8_t>(N);

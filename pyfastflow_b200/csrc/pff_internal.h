@@ -14,6 +14,20 @@ namespace pff {
 extern std::atomic<long long> g_launches;
 inline void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// Timing probes (pff_probe_enable / pff_probe_read): PFF_PROBED(name, stream, launch)
+// brackets `launch` with events on `stream` while probes are armed.
+struct ProbeMark {
+    int slot, idx;
+};
+ProbeMark probe_begin(const char *name, cudaStream_t st);
+void probe_end(ProbeMark m, cudaStream_t st);
+#define PFF_PROBED(name, st, ...)                                 \
+    do {                                                          \
+        const ::pff::ProbeMark _pm = ::pff::probe_begin(name, st); \
+        __VA_ARGS__;                                              \
+        ::pff::probe_end(_pm, st);                                \
+    } while (0)
+
 void set_error(const char *fmt, ...);
 void clear_error();
 

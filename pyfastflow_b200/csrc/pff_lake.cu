@@ -1185,13 +1185,17 @@ static void l_tile_terminal(const int32_t *rec, int32_t *J, int32_t *R, int *pit
                             cudaStream_t st)
 {
     dim3 gr(div_up(g.nx, TILE_W), div_up(g.ny, TILE_H));
-    { k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g, nullptr, nullptr); count_launch(); }
+    PFF_PROBED("k_tile_terminal<grid>", st,
+               k_tile_terminal<MODE><<<gr, TILE_THREADS, 0, st>>>(rec, J, R, pits, info, g, nullptr, nullptr));
+    count_launch();
 }
 template <int MODE>
 static void l_tile_terminal_list(const int32_t *rec, int32_t *J, int32_t *R, int *info, const Grid &g,
                                  const int *tiles, const int *ntiles, int grid, cudaStream_t st)
 {
-    { k_tile_terminal<MODE><<<grid, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles, ntiles); count_launch(); }
+    PFF_PROBED("k_tile_terminal<list>", st,
+               k_tile_terminal<MODE><<<grid, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles, ntiles));
+    count_launch();
 }
 template <int MODE>
 static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, const int32_t *rec,
@@ -1742,6 +1746,21 @@ struct RREntry {
     RRKernelCounts kc{};
 };
 
+// Whether pff_reroute_flow runs its outer loop from a device-driven graph (default)
+// or from the host loop; PFF_REROUTE_NO_GRAPH in the environment turns the default
+// off, pff_reroute_use_graphs changes it at run time.
+static std::atomic<int> g_rr_graphs{-1};
+static bool rr_graphs_on()
+{
+    int v = g_rr_graphs.load();
+    if (v < 0) {
+        int fresh = getenv("PFF_REROUTE_NO_GRAPH") != nullptr ? 0 : 1;
+        if (!g_rr_graphs.compare_exchange_strong(v, fresh)) return g_rr_graphs.load() != 0;
+        v = fresh;
+    }
+    return v != 0;
+}
+
 // Launch the device-driven loop for these buffers (a graph built and kept on the
 // first call with them), then read its final state (one synchronisation).
 // Returns PFF_ERR_UNSUPPORTED when graphs cannot be built here.
@@ -1753,8 +1772,7 @@ static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec
     static std::mutex mu;
     static RREntry cache[8];
     static int next = 0;
-    static bool disabled = getenv("PFF_REROUTE_NO_GRAPH") != nullptr;  // diagnostics: force the host loop
-    if (disabled) return PFF_ERR_UNSUPPORTED;
+    if (!rr_graphs_on()) return PFF_ERR_UNSUPPORTED;
     (void)workspace;
     (void)workspace_bytes;
     int dev = 0;
@@ -2066,4 +2084,12 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
     PFF_CUDA(cudaMemsetAsync(w.dirty, 0, (size_t)ntiles, st));
     return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag, tag_,
                              carve, g, w, 0, 0, !carve, 0, n_outer_out, st);
+}
+
+extern "C" int pff_reroute_use_graphs(int on)
+{
+    clear_error();
+    const int prev = rr_graphs_on() ? 1 : 0;
+    g_rr_graphs.store(on != 0 ? 1 : 0);
+    return prev;
 }

@@ -52,6 +52,38 @@ def test_fill_z_add_delta(orc, cuda, mode):
     assert np.array_equal(bits(host(z_)), bits(z_o))
 
 
+def test_fill_arbitrary_pointers(orc, cuda):
+    """Fill rounds on receivers that are not a forest: random pointers (cycles of
+    every length, self-pointers made by jumping around a cycle) and NaN heights.
+    The packed rounds read zh at such self-pointers; bit-exact against the oracle,
+    including both receiver buffers."""
+    torch = cuda
+    from pyfastflow_b200 import flow
+
+    rng = np.random.default_rng(21)
+    for n in (2, 3, 1000, 70001):
+        zh = (rng.random(n) * 100).astype(np.float32)
+        zh[rng.random(n) < 0.01] = np.nan
+        h = (rng.random(n) * 0.3).astype(np.float32)
+        rcv = rng.integers(0, n, n).astype(np.int32)
+        rcv[rng.random(n) < 0.2] = rng.integers(0, n)  # one cell with many donors
+        roots = rng.random(n) < 0.1
+        rcv[roots] = np.flatnonzero(roots)
+        zd, hd = dev(torch, zh), dev(torch, h)
+        z_ = torch.zeros_like(zd)
+        r_ = torch.zeros(n, dtype=torch.int32, device="cuda")
+        r__ = torch.zeros(n, dtype=torch.int32, device="cuda")
+        flow.fill_z_add_delta(zd, hd, z_, dev(torch, rcv), r_, r__, epsilon=1e-3)
+        zo, ho, z_o = orc.fill_z_add_delta(zh.copy(), h.copy(), rcv, eps=1e-3)
+        assert np.array_equal(bits(host(zd)), bits(zo)), n
+        assert np.array_equal(bits(host(hd)), bits(ho)), n
+        assert np.array_equal(bits(host(z_)), bits(z_o)), n
+        jumped = rcv.copy()
+        for _ in range(int(np.ceil(np.log2(n)))):
+            jumped = jumped[jumped]
+        assert np.array_equal(host(r_), jumped) and np.array_equal(host(r__), jumped), n
+
+
 @pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_diffuse(orc, cuda, mode):
     torch = cuda
@@ -75,6 +107,35 @@ def test_diffuse(orc, cuda, mode):
         orc.diffuse_q(zh, Qo, og, 10.0, 1e-5)
     assert np.array_equal(bits(host(Qd)), bits(Qo))
     assert np.array_equal(bits(host(tmp)), bits(Qo))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_diffuse_shapes_and_sweeps(orc, cuda, mode):
+    """All sweeps of one call in one tiled pass (64 x 16 tiles, halo = sweeps): grids
+    narrower than the halo, ragged tile edges, 1-8 sweeps and 9 (the per-sweep path),
+    each bit-exact against the oracle's serial sweeps."""
+    torch = cuda
+    from pyfastflow_b200 import constants as cte
+    from pyfastflow_b200.graphflood import diffuse_Q_constant_prec
+
+    cases = [(3, 3, 5), (3, 40, 8), (70, 3, 5), (5, 7, 2), (65, 17, 1), (129, 33, 5), (200, 50, 8),
+             (64, 16, 3), (90, 45, 9)]
+    for nx, ny, ns in cases:
+        rng = np.random.default_rng(nx * 1000 + ny + mode)
+        zh = synthetic.spectral_dem(nx, ny, 11, relief=20.0).ravel() if min(nx, ny) > 8 else \
+            (rng.random(nx * ny) * 5).astype(np.float32)
+        zh[rng.random(nx * ny) < 0.05] = zh.min()  # flats and pits: cells with no outflow
+        og = orc.Grid(nx, ny, mode)
+        Q = (rng.random(nx * ny) * 10).astype(np.float32)
+        cte.NX, cte.NY, cte.DX, cte.BOUND_MODE, cte.PREC = nx, ny, 7.5, mode, 2e-5
+        cte.boundaries = None
+        Qd, tmp = dev(torch, Q), torch.zeros(nx * ny, dtype=torch.float32, device="cuda")
+        diffuse_Q_constant_prec(dev(torch, zh), Qd, tmp, nsweeps=ns)
+        Qo = Q.copy()
+        for _ in range(ns):
+            orc.diffuse_q(zh, Qo, og, 7.5, 2e-5)
+        assert np.array_equal(bits(host(Qd)), bits(Qo)), (nx, ny, ns)
+        assert np.array_equal(bits(host(tmp)), bits(Qo)), (nx, ny, ns)
 
 
 def test_manning_core(orc, cuda):

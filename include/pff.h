@@ -37,6 +37,7 @@ extern "C" {
 #define PFF_ERR_CUDA 2       /* CUDA runtime error (launch or copy) */
 #define PFF_ERR_NOCONV 3     /* iteration cap reached before convergence */
 #define PFF_ERR_WORKSPACE 4  /* workspace too small */
+#define PFF_ERR_UNAVAILABLE 5 /* this path is not available here (e.g. CUDA graphs switched off) */
 
 /* Library version (major*10000 + minor*100 + patch). */
 int pff_version(void);
@@ -161,6 +162,48 @@ int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, 
                      int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int carve, int nx,
                      int ny, int bound_mode, const uint8_t *codes, void *workspace,
                      size_t workspace_bytes, int *n_outer_out, void *stream);
+/* pff_reroute_flow (carve) split at its one host synchronisation, so that a caller can
+ * queue more work behind the reroute before it looks at the result (no reference
+ * counterpart; the Flooder's pipelined loop uses it).
+ *   - pff_reroute_flow_async launches the device-driven outer loop and returns; the
+ *     graph's last node copies its final state (9 ints) into ctl_out (device memory, or
+ *     pinned host memory, which it writes through its unified address).
+ *     Returns PFF_ERR_UNAVAILABLE where that loop cannot run (graphs switched off by
+ *     pff_reroute_use_graphs / PFF_REROUTE_NO_GRAPH, or not supported).
+ *   - pff_reroute_flow_finish takes a host copy of those 9 ints, once the launch has
+ *     completed, and does what pff_reroute_flow does after its graph: nothing if the
+ *     loop finished on the device (ctl[3] = 1 no pits, or 2 done), the reference's
+ *     steps on the host if it stopped for them (3, 4; synchronises), an error
+ *     otherwise.  Same buffers and workspace as the async call; *n_outer_out as in
+ *     pff_reroute_flow.
+ * Together they leave every buffer as one pff_reroute_flow(carve = 1) call does. */
+int pff_reroute_flow_async(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                           float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
+                           int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int nx, int ny,
+                           int bound_mode, const uint8_t *codes, void *workspace, size_t workspace_bytes,
+                           int *ctl_out, void *stream);
+int pff_reroute_flow_finish(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                            float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
+                            int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int nx, int ny,
+                            int bound_mode, const uint8_t *codes, void *workspace, size_t workspace_bytes,
+                            const int *ctl_host, int *n_outer_out, void *stream);
+/* A region of work that runs only after a finished asynchronous reroute (no reference
+ * counterpart).  pff_guard_begin starts capturing `stream` (not the legacy default
+ * stream) into the body of a conditional graph; everything the caller issues on it
+ * until pff_guard_end is recorded, not run.  pff_guard_launch runs the graph: its
+ * first node reads ctl[3] (the state words of pff_reroute_flow_async) and the
+ * optional flag, and the body runs when the state is 1 or 2 and *flag is 0.
+ * pff_guard_destroy frees it.  At most 1024 regions at a time. */
+int pff_guard_begin(const int *ctl, const int *flag, void *stream, int *id);
+int pff_guard_end(int id, void *stream);
+int pff_guard_launch(int id, void *stream);
+int pff_guard_destroy(int id);
+/* out_dev[0] and out_host[0] = val[0], each if non-NULL: one small kernel; out_host may be
+ * pinned host memory (written through its unified address, no copy engine). */
+int pff_value_store(const float *val, float *out_dev, float *out_host, void *stream);
+/* flag[0] = 1 if (double)val[0] / div < thr, else 0 (device values; the host's
+ * residual test float(value) / dt < threshold made on the device, in double). */
+int pff_residual_flag(const float *val, double div, double thr, int *flag, void *stream);
 
 /* Basin labels of a receiver forest: lakeflow.py:82-101 basin_identification
  * (bid = root+1, or 0 when the root can leave the domain).  rec_ is scratch (N). */
@@ -229,6 +272,15 @@ int pff_diffuse_q(const float *zh, float *Q, float *temp, int nsweeps, int nx, i
 int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t *rec, const float *Q, int N,
                         float dx, float dx2, float manning, float edgesw, float dt,
                         const float *h_ref, float *dhmax, void *stream);
+/* pff_graphflood_core in one pass, for a caller that holds a copy of zh in zf (the
+ * Flooder: the fill leaves the filled surface in both z_ and zh, and nothing changes
+ * either before the Manning update).  The slope reads zf, so zh is updated in the
+ * same pass; results are pff_graphflood_core's, bit for bit, when zf equals zh.
+ * zf must not alias zh.  Replaces the two loops of gf_hydrodynamics.py:79-129 inside
+ * Flooder.run_graphflood (gf_fields.py:141). */
+int pff_graphflood_core_filled(float *h, float *zh, const float *zf, float *dh, const int32_t *rec,
+                               const float *Q, int N, float dx, float dx2, float manning, float edgesw,
+                               float dt, const float *h_ref, float *dhmax, void *stream);
 
 /* out[0] = max |a - b| (maxed into its current value as unsigned bits, so a NaN
  * difference wins), out[1] += sum |a - b| (f32, unspecified order).  Zero out first.

@@ -32,6 +32,17 @@ def stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+def resolve_device(device):
+    """torch.device with an explicit index ("cuda" -> the current CUDA device): tensors
+    always report an index, so comparisons need one."""
+    if device is None:
+        return None
+    device = torch.device(device)
+    if device.type == "cuda" and device.index is None and torch.cuda.is_available():
+        device = torch.device("cuda", torch.cuda.current_device())
+    return device
+
+
 class Scratch:
     """Grow-only device scratch buffer (one per owner), handed to the C ABI as workspace."""
 
@@ -39,7 +50,11 @@ class Scratch:
         self.buf = None
 
     def get(self, nbytes: int, device=None) -> tuple[int, int]:
+        """The buffer (at least nbytes) as (pointer, size).  It is reallocated only when it
+        is too small or on another device, so graphs that captured its address stay valid;
+        "cuda" without an index means the current device."""
         nbytes = max(int(nbytes), 256)
+        device = resolve_device(device)
         if self.buf is None or self.buf.numel() < nbytes or (device is not None and self.buf.device != device):
             self.buf = torch.empty(nbytes, dtype=torch.uint8, device=device or "cuda")
         return self.buf.data_ptr(), self.buf.numel()

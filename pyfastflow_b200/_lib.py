@@ -23,6 +23,14 @@ SIGNATURES = {
     "pff_probe_enable": (_i32, [_i32]),
     "pff_probe_read": (_i32, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "pff_reroute_use_graphs": (_i32, [_i32]),
+    "pff_reroute_flow_async": (_i32, [_vp] * 12 + [_i32, _i32, _i32, _vp, _vp, _sz, _vp, _vp]),
+    "pff_reroute_flow_finish": (_i32, [_vp] * 12 + [_i32, _i32, _i32, _vp, _vp, _sz, _vp, _vp, _vp]),
+    "pff_guard_begin": (_i32, [_vp, _vp, _vp, _vp]),
+    "pff_guard_end": (_i32, [_i32, _vp]),
+    "pff_guard_launch": (_i32, [_i32, _vp]),
+    "pff_guard_destroy": (_i32, [_i32]),
+    "pff_residual_flag": (_i32, [_vp, _f64, _f64, _vp, _vp]),
+    "pff_value_store": (_i32, [_vp, _vp, _vp, _vp]),
     "pff_set_device": (_i32, [_i32]),
     "pff_compute_receivers": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, _vp]),
     "pff_compute_receivers_stochastic": (_i32, [_vp, _vp, _vp, _i32, _i32, _f32, _i32, _vp, C.c_uint64, _vp]),
@@ -48,6 +56,7 @@ SIGNATURES = {
     "pff_diffuse_workspace_bytes": (_sz, [_i32]),
     "pff_diffuse_q": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _f32, _f32, _i32, _vp, _vp, _sz, _vp]),
     "pff_graphflood_core": (_i32, [_vp] * 5 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
+    "pff_graphflood_core_filled": (_i32, [_vp] * 6 + [_i32] + [_f32] * 5 + [_vp, _vp, _vp]),
     "pff_abs_diff_stats": (_i32, [_vp, _vp, _i32, _vp, _vp]),
     "pff_archive_workspace_bytes": (_sz, [_i32]),
     "pff_tree_accum_down": (_i32, [_vp, _vp, _vp, _i32, _vp, _sz, _vp]),

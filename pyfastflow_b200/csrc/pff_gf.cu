@@ -37,26 +37,37 @@ __global__ void __launch_bounds__(256) k_fill_pack(const float *__restrict__ zh,
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const int r = rcv[i];
+    int r = rcv[i];
+    if ((unsigned)r >= (unsigned)N) r = i;  // an out-of-range receiver: no read outside the records
     A[i] = make_uint2((uint32_t)r | (r == i ? FILL_ROOT : 0u), __float_as_uint(zh[i]));
 }
 
-__global__ void __launch_bounds__(256) k_fill_round_packed(const float *__restrict__ zh, const uint2 *__restrict__ A,
-                                                           uint2 *__restrict__ B, float inc, int N)
+__device__ __forceinline__ uint2 fill_step(const float *__restrict__ zh, int i, uint2 me, uint2 at, float inc)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const uint2 me = A[i];
     const int r = (int)(me.x & ~FILL_ROOT);
-    const uint2 at = A[r];
     const int rr = (int)(at.x & ~FILL_ROOT);
     const float zi = __uint_as_float(me.y), zr = __uint_as_float(at.y);
-    B[i].x = (uint32_t)rr | (me.x & FILL_ROOT);           // :29
     float zn;
     if (i == r) zn = zi;
     else if (rr == r && zi > ((at.x & FILL_ROOT) ? zr : zh[r])) zn = zi;  // :32
-    else zn = fmaxf(zi, __fadd_rn(zr, inc));              // :36
-    B[i].y = __float_as_uint(zn);
+    else zn = fmaxf(zi, __fadd_rn(zr, inc));                              // :36
+    return make_uint2((uint32_t)rr | (me.x & FILL_ROOT), __float_as_uint(zn));  // :29
+}
+
+// two cells per thread (i and i + 256 in a block's 512): both gathers in flight at once
+__global__ void __launch_bounds__(256) k_fill_round_packed(const float *__restrict__ zh, const uint2 *__restrict__ A,
+                                                           uint2 *__restrict__ B, float inc, int N)
+{
+    const int i0 = blockIdx.x * 512 + threadIdx.x, i1 = i0 + 256;
+    if (i1 < N) {
+        const uint2 m0 = A[i0], m1 = A[i1];
+        const uint2 a0 = A[m0.x & ~FILL_ROOT], a1 = A[m1.x & ~FILL_ROOT];
+        B[i0] = fill_step(zh, i0, m0, a0, inc);
+        B[i1] = fill_step(zh, i1, m1, a1, inc);
+    } else if (i0 < N) {
+        const uint2 m0 = A[i0];
+        B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc);
+    }
 }
 
 // the packed result to z_ and both receiver buffers (:39-40), then, if h is given,
@@ -224,15 +235,18 @@ __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__
                 const float zi = zs[z];
                 const float zn[4] = {zs[z - ZX], zs[z - 1], zs[z + 1], zs[z + ZX]};
                 float sk[4], sums = 0.f;
+                // max(0, (zi - zj) / dx) is +0 unless zi > zj (NaN compares false and
+                // max(0, NaN) is 0), and 0 / sums is +0 for the sums > 0 of a source:
+                // only the descending links divide
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    sk[k] = fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zn[k]), dx));
+                    sk[k] = zi > zn[k] ? fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zn[k]), dx)) : 0.f;
                     sums = __fadd_rn(sums, sk[k]);
                 }
                 if (sums != 0.f) {
                     f |= 2;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) wk[k] = __fdiv_rn(sk[k], sums);
+                    for (int k = 0; k < 4; ++k) wk[k] = sk[k] != 0.f ? __fdiv_rn(sk[k], sums) : 0.f;
                 }
             }
         }
@@ -337,7 +351,8 @@ __global__ void __launch_bounds__(256) k_core1(float *h, const float *__restrict
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const int r = rec[i];
+    int r = rec[i];
+    if ((unsigned)r >= (unsigned)N) r = i;  // an out-of-range receiver reads nothing: the edge slope
     float tS = edgesw;
     if (r != i) tS = fmaxf(__fdiv_rn(__fsub_rn(zh[i], zh[r]), dx), 1e-4f);
     float Qo = __fmul_rn(dx, pow53(h[i]));
@@ -366,6 +381,50 @@ __global__ void __launch_bounds__(256) k_core2(float *h, float *zh, const float 
     if (!dhmax || !href) return;
     // |dh| >= 0 or NaN: as unsigned bits, NaN sorts above every finite value;
     // warp max, block max, then one atomic per block
+    unsigned mu = __float_as_uint(m);
+    for (int o = 16; o; o >>= 1) mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    __shared__ unsigned wm[8];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mu;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned b = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) b = max(b, wm[k]);
+        if (b) atomicMax(reinterpret_cast<unsigned int *>(dhmax), b);
+    }
+}
+
+// Both Manning loops in one pass, for a caller whose zf holds a copy of zh (the
+// filled surface the fill leaves in z_ and in zh): the slope reads zf, which no
+// thread writes, so zh can be updated in the same pass.  Per cell the operations
+// of k_core1 then k_core2, in their order.
+__global__ void __launch_bounds__(256) k_core_fused(float *h, float *zh, const float *__restrict__ zf, float *dh,
+                                                    const int32_t *__restrict__ rec, const float *__restrict__ Q,
+                                                    int N, float dx, float dx2, float manning, float edgesw, float dt,
+                                                    const float *__restrict__ href, float *dhmax)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float m = 0.f;
+    if (i < N) {
+        int r = rec[i];
+        if ((unsigned)r >= (unsigned)N) r = i;  // as in k_core1
+        const float zi = zf[i];
+        float tS = edgesw;
+        if (r != i) tS = fmaxf(__fdiv_rn(__fsub_rn(zi, zf[r]), dx), 1e-4f);
+        const float hi = h[i];
+        float Qo = __fmul_rn(dx, pow53(hi));
+        Qo = __fdiv_rn(Qo, manning);
+        Qo = __fmul_rn(Qo, __fsqrt_rn(tS));
+        float tdh = __fdiv_rn(__fsub_rn(Q[i], Qo), dx2);
+        tdh = __fmul_rn(tdh, dt);
+        const float h1 = __fadd_rn(hi, tdh);
+        if (h1 < 0.f) tdh = __fadd_rn(tdh, h1);
+        dh[i] = tdh;
+        const float hn = __fadd_rn(h1, tdh);  // k_core2
+        h[i] = hn;
+        zh[i] = __fadd_rn(zi, tdh);
+        if (dhmax && href) m = fabsf(__fsub_rn(hn, href[i]));
+    }
+    if (!dhmax || !href) return;
     unsigned mu = __float_as_uint(m);
     for (int o = 16; o; o >>= 1) mu = max(mu, __shfl_xor_sync(0xffffffffu, mu, o));
     __shared__ unsigned wm[8];
@@ -436,7 +495,7 @@ static uint2 *fill_rounds(const float *zh, const int32_t *receivers, void *works
     int nr = 0;
     for (long long p = 1; p < N; p <<= 1) ++nr;
     for (int it = 0; it < nr; ++it) {
-        PFF_PROBED("k_fill_round_packed", st, k_fill_round_packed<<<div_up(N, 256), 256, 0, st>>>(zh, a, b, inc(it), N));
+        PFF_PROBED("k_fill_round_packed", st, k_fill_round_packed<<<div_up(N, 512), 256, 0, st>>>(zh, a, b, inc(it), N));
         count_launch();
         std::swap(a, b);
     }
@@ -618,6 +677,23 @@ extern "C" int pff_graphflood_core(float *h, float *zh, float *dh, const int32_t
     { k_core1<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, rec, Q, N, dx, dx2, manning, edgesw, dt); count_launch(); }
     { k_core2<<<div_up(N, 256), 256, 0, st>>>(h, zh, dh, h_ref, dhmax, N); count_launch(); }
     return check_cuda("pff_graphflood_core");
+}
+
+extern "C" int pff_graphflood_core_filled(float *h, float *zh, const float *zf, float *dh, const int32_t *rec,
+                                          const float *Q, int N, float dx, float dx2, float manning, float edgesw,
+                                          float dt, const float *h_ref, float *dhmax, void *stream)
+{
+    clear_error();
+    if (N <= 0 || !h || !zh || !zf || !dh || !rec || !Q || zf == zh) {
+        set_error("pff_graphflood_core_filled: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    cudaStream_t st = S(stream);
+    PFF_PROBED("k_core_fused", st,
+               k_core_fused<<<div_up(N, 256), 256, 0, st>>>(h, zh, zf, dh, rec, Q, N, dx, dx2, manning, edgesw, dt,
+                                                             h_ref, dhmax));
+    count_launch();
+    return check_cuda("pff_graphflood_core_filled");
 }
 
 extern "C" int pff_abs_diff_stats(const float *a, const float *b, int N, float *out, void *stream)

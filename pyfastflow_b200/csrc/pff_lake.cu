@@ -473,12 +473,35 @@ __global__ void k_basin_reset_list(long long *saddle, long long *outlet, int32_t
 constexpr int SAD_ROWS = 32;
 constexpr int SAD_AHEAD = 4;  // rows loaded per group (SAD_ROWS is a multiple)
 
+// The saddle candidate of a border cell goes to atomicMin(saddle + bi, key) (pass 2).
+// In the border-list pass, where most lanes hold a candidate and neighbouring list
+// entries share basins, saddle_min_warp makes that one atomic per basin per warp
+// (in the N-wide strip pass it cost more than it saved): the lanes holding a
+// candidate group by basin (match.any), take the group's minimum key as two 32-bit
+// reductions (the key's signed order is the unsigned order of key ^ 2^63: high
+// words first, then the low words of the lanes that hold the minimal high word),
+// and the group's first lane applies it.  The minimum over the same keys: the
+// saddle is the one the per-cell atomics produce.
+__device__ __forceinline__ void saddle_min_warp(long long *saddle, int bi, long long key, bool has)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, has);
+    if (!has) return;
+    const unsigned peers = __match_any_sync(act, bi);
+    const unsigned long long u = (unsigned long long)key ^ 0x8000000000000000ull;
+    const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+    const unsigned mh = __reduce_min_sync(peers, hi);
+    const unsigned ml = __reduce_min_sync(peers, hi == mh ? lo : 0xffffffffu);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1)
+        atomicMin(saddle + bi, (long long)((((unsigned long long)mh << 32) | ml) ^ 0x8000000000000000ull));
+}
+
+// Passes 1-2 for one cell; the saddle candidate (if any) is returned in key/has.
 // Returns 0 for a cell off every border, 1 for a border cell of the outlet
 // basin 0, 2 for a border cell of a pit basin.
 template <int MODE>
 __device__ __forceinline__ int saddle_cell(int i, int row, int col, const Grid &g, int bi, float zi, const int (&jn)[4],
                                            const int (&bn)[4], const float (&zn)[4], uint8_t *is_border, float *zp,
-                                           long long *saddle)
+                                           long long &key, bool &has)
 {
     bool border = false;
     float zmin = 1e9f;
@@ -497,7 +520,8 @@ __device__ __forceinline__ int saddle_cell(int i, int row, int col, const Grid &
         const long long c = pack_key(zpi, bn[k]);
         res = c < res ? c : res;
     }
-    if (res != iv) atomicMin(saddle + bi, res);
+    key = res;
+    has = res != iv;
     return bi != 0 ? 2 : 1;
 }
 
@@ -552,6 +576,8 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
             int bl = __shfl_up_sync(0xffffffffu, bc, 1), br = __shfl_down_sync(0xffffffffu, bc, 1);
             float zl = __shfl_up_sync(0xffffffffu, zc, 1), zr = __shfl_down_sync(0xffffffffu, zc, 1);
             int listed = 0;  // saddle_cell's code
+            long long key = 0;
+            bool has = false;
             if (incol) {
                 const bool interior = MODE != 3 && rw > 0 && rw < ny - 1 && col > 0 && col < nx - 1;
                 if (interior) {
@@ -561,7 +587,7 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
                     const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
                     const int bn[4] = {ba, bl, br, bb};
                     const float zn[4] = {za, zl, zr, zb};
-                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, key, has);
                 } else if (can_leave<MODE>(g, i, rw, col)) {
                     zp[i] = zc;
                 } else {
@@ -573,9 +599,10 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
                         bn[k] = jn[k] != -1 ? bid[jn[k]] : 0;
                         zn[k] = jn[k] != -1 ? z[jn[k]] : 0.f;
                     }
-                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, saddle);
+                    listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, key, has);
                 }
             }
+            if (has) atomicMin(saddle + bc, key);
             // every border cell, the pit-basin ones marked by the sign bit
             const unsigned m = __ballot_sync(0xffffffffu, listed != 0);
             if (listed) buf[wib][nb + __popc(m & ((1u << lane) - 1u))] = listed == 2 ? (i | (int)0x80000000) : i;
@@ -624,7 +651,9 @@ __global__ void __launch_bounds__(256) k_saddle_p12_border(const int32_t *__rest
     const int trips = (n + stride - 1) / stride;
     for (int k = 0; k < trips; ++k) {
         const int idx = k * stride + blockIdx.x * 256 + threadIdx.x;
-        int code = 0, i = -1;
+        int code = 0, i = -1, bi = 0;
+        long long key = 0;
+        bool has = false;
         if (idx < n) {
             i = aprev[idx];
             const int row = i / g.nx, col = i - row * g.nx;
@@ -637,8 +666,10 @@ __global__ void __launch_bounds__(256) k_saddle_p12_border(const int32_t *__rest
                 zn[q] = jn[q] != -1 ? z[jn[q]] : 0.f;
             }
             // an outlet is never listed (its z' is z and it has no border status)
-            code = saddle_cell<MODE>(i, row, col, g, bid[i], z[i], jn, bn, zn, is_border, zp, saddle);
+            bi = bid[i];
+            code = saddle_cell<MODE>(i, row, col, g, bi, z[i], jn, bn, zn, is_border, zp, key, has);
         }
+        saddle_min_warp(saddle, bi, key, has);
         block_append<256>(code != 0, i, anext, nanext);
         block_append<256>(code == 2, i, blist, nblist);
     }
@@ -944,12 +975,37 @@ __global__ void k_relabel_init(int32_t *fin, const int32_t *__restrict__ bid, co
     }
 }
 
-// fin[b] = fin[fin[b]] over the pit list, all rounds in one cooperative launch.
+// fin[b] = fin[fin[b]] over the pit list.  Up to RJ_BLOCK pits one CTA does every
+// round, with block barriers (its own global writes are visible to it after each);
+// longer lists take the cooperative launch with grid-wide barriers.  Each kernel
+// reads the count on the device and leaves the other's lists.
+// Inside the reroute graph the block kernel also sets a conditional handle, so the
+// cooperative launch (whose launch alone costs about 10 us) runs only for long lists.
+constexpr int RJ_BLOCK = 16384;
+__global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const int *__restrict__ pits, const int *np,
+                                                            cudaGraphConditionalHandle hj, int set)
+{
+    const int n = *np;
+    if (set && threadIdx.x == 0) cudaGraphSetConditional(hj, n > RJ_BLOCK ? 1u : 0u);
+    if (n > RJ_BLOCK) return;
+    for (int r = 0; r < 32; ++r) {
+        bool ch = false;
+        for (int k = threadIdx.x; k < n; k += 1024) {
+            const int b = pits[k] + 1;
+            const int x = fin[b];
+            const int y = fin[x];
+            if (y != x) { fin[b] = y; ch = true; }
+        }
+        if (!__syncthreads_or(ch)) break;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_relabel_jump_coop(int32_t *fin, const int *__restrict__ pits, const int *np,
                                                            int *flags)
 {
     cooperative_groups::grid_group grid = cooperative_groups::this_grid();
     const int n = *np;
+    if (n <= RJ_BLOCK) return;  // uniform over the grid: no block reaches a grid barrier
     for (int r = 0; r < 32; ++r) {
         bool ch = false;
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -966,9 +1022,11 @@ __global__ void __launch_bounds__(256) k_relabel_jump_coop(int32_t *fin, const i
 
 // four cells per thread; label 0 (outlet basins) never changes.  The same pass
 // makes rec_ = rec on the carved cells (k_sync_tagged's copy, :526).
+// The carve tags are consumed here: tagged cells are cleared in tag and tag_ (the
+// carve tags the same cells in both), so the next carve needs no N-wide clear.
 __global__ void __launch_bounds__(256) k_relabel(int32_t *bid, const int32_t *__restrict__ fin, int32_t *rec_,
-                                                 const int32_t *__restrict__ rec, const uint8_t *__restrict__ tag,
-                                                 int N, int vec)
+                                                 const int32_t *__restrict__ rec, uint8_t *tag, uint8_t *tag_, int N,
+                                                 int vec)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = 4 * q;
@@ -985,10 +1043,18 @@ __global__ void __launch_bounds__(256) k_relabel(int32_t *bid, const int32_t *__
         if (t.y) rec_[i + 1] = rec[i + 1];
         if (t.z) rec_[i + 2] = rec[i + 2];
         if (t.w) rec_[i + 3] = rec[i + 3];
+        if (t.x | t.y | t.z | t.w) {
+            reinterpret_cast<uchar4 *>(tag)[q] = make_uchar4(0, 0, 0, 0);
+            for (int k = i; k < i + 4; ++k) tag_[k] = 0;
+        }
     } else {
         for (int k = i; k < N && k < i + 4; ++k) {
             if (bid[k]) bid[k] = fin[bid[k]];
-            if (tag[k]) rec_[k] = rec[k];
+            if (tag[k]) {
+                rec_[k] = rec[k];
+                tag[k] = 0;
+                tag_[k] = 0;
+            }
         }
     }
 }
@@ -1536,7 +1602,12 @@ static int coop_blocks_for(const void *fn)
 // iteration 0 (labels come from the prologue); otherwise it starts with the basin
 // relabelling and the dirty tiles' terminals that the previous iteration's
 // decision asked for.
-static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
+static int rr_cond(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t *body);
+static int rr_handle(cudaStream_t s, cudaGraphConditionalHandle *h);
+
+// One outer iteration, captured on s (inside the reroute graph); aux captures the
+// body of the conditional cooperative relabel launch.
+static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s, cudaStream_t aux)
 {
     const Grid &g = A.g;
     const RerouteWs &w = A.w;
@@ -1548,7 +1619,7 @@ static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
     const int ntx = div_up(nx, TILE_W), ntiles = ntx * div_up(g.ny, TILE_H);
     int *np = w.ctr + 16 * par, *np_next = w.ctr + 16 * (par ^ 1);
     if (!first) {
-        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, s>>>(A.bid, w.fin, A.rec_, A.rec, A.tag, N,
+        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, s>>>(A.bid, w.fin, A.rec_, A.rec, A.tag, A.tag_, N,
                                                          ((uintptr_t)A.bid & 15) == 0 && ((uintptr_t)A.tag & 3) == 0); count_launch(); }
         PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, A.rec_, A.rec__, w.R, np_next, g, w.tiles, w.ctr + 44,
                           std::min(ntiles, grid), s);
@@ -1561,8 +1632,10 @@ static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
     PFF_MODE_DISPATCH(g.mode, l_saddle_lists, A.bid, A.isb, A.zp, A.sad, A.snode, A.out, w.inv, A.z, g, w.pits[par],
                       np, w.blist, w.ctr + 40, first ? nullptr : w.alist[par ^ 1], w.ctr + 50 + (par ^ 1),
                       w.alist[par], w.ctr + 50 + par, grid, s);
-    PFF_CUDA(cudaMemsetAsync(A.tag, 0, (size_t)N, s));
-    PFF_CUDA(cudaMemsetAsync(A.tag_, 0, (size_t)N, s));
+    if (first) {  // later iterations: k_relabel cleared the previous carve's tags
+        PFF_CUDA(cudaMemsetAsync(A.tag, 0, (size_t)N, s));
+        PFF_CUDA(cudaMemsetAsync(A.tag_, 0, (size_t)N, s));
+    }
     { k_carve_segments<<<nsm * 4, 32 * SEG_WARPS, 0, s>>>(A.snode, A.rec_, A.rec__, w.pits[par], np, N, w.segs,
                                                            w.ctr + 41, N, w.ctr + 43); count_launch(); }
     { k_carve_walk<<<nsm * 4, WALK_THREADS, 0, s>>>(A.rec_, A.rec, A.tag, A.tag_, w.segs, w.ctr + 41, N, nx, g.ny,
@@ -1578,9 +1651,20 @@ static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
     if (!coop_relabel) coop_relabel = coop_blocks_for((const void *)k_relabel_jump_coop);
     int *plist = w.pits[par];
     int32_t *fin = w.fin;
+    cudaGraphConditionalHandle hj;
+    PFF_TRY(rr_handle(s, &hj));
+    { k_relabel_jump_block<<<1, 1024, 0, s>>>(fin, plist, np, hj, 1); count_launch(); }
+    cudaGraph_t jbody = nullptr;
+    PFF_TRY(rr_cond(s, hj, cudaGraphCondTypeIf, &jbody));
+    PFF_CUDA(cudaStreamBeginCaptureToGraph(aux, jbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     void *args[] = {&fin, &plist, &np, &flags};
-    PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, s));
-    count_launch();
+    // not counted: the graph's launch tally counts it once per replay, and it runs
+    // only for pit lists longer than RJ_BLOCK
+    const cudaError_t le = cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, aux);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(aux, &captured);
+    PFF_CUDA(le);
+    PFF_CUDA(ee);
     PFF_CUDA(cudaMemsetAsync(w.ctr + 49, 0, sizeof(int), s));
     { k_relabel_check<<<grid, B, 0, s>>>(w.fin, A.out, w.pits[par], np, N, w.ctr + 49); count_launch(); }
     return check_cuda("reroute iteration");
@@ -1589,7 +1673,7 @@ static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s)
 // streams used to capture the graph's nested bodies (one per nesting depth)
 static cudaStream_t rr_capture_stream(int dev, int depth)
 {
-    static cudaStream_t streams[64][5];
+    static cudaStream_t streams[64][10];
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
     if (!streams[dev][depth]) cudaStreamCreateWithFlags(&streams[dev][depth], cudaStreamNonBlocking);
@@ -1627,10 +1711,18 @@ static int rr_handle(cudaStream_t s, cudaGraphConditionalHandle *h)
 
 struct RRKernelCounts {
     long long pro, a, b0, it2;  // kernels in the prologue, body A, iteration 0, a parity-1 iteration + decide
+    long long tail;             // the state copy at the end (graphs built for pff_reroute_flow_async)
 };
 
+// the final state words (RR_CTL .. +8) into the caller's device buffer
+// (out may be pinned host memory, written through its unified address)
+__global__ void k_rr_ctl_copy(const int *ctl, int *out)
+{
+    if (threadIdx.x < 9) ((volatile int *)out)[threadIdx.x] = ctl[threadIdx.x];
+}
+
 // Capture the whole graph.  Every capture begun here is ended on every path.
-static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *kc)
+static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *kc, int *ctl_out)
 {
     const Grid &g = A.g;
     const RerouteWs &w = A.w;
@@ -1689,7 +1781,7 @@ static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *k
         l0 = g_launches.load();
         if ((rc = rr_cond(s[1], hb, cudaGraphCondTypeIf, &body[2]))) break;
         if ((rc = begin(2))) break;
-        if ((rc = rr_iteration(A, 0, true, s[2]))) break;
+        if ((rc = rr_iteration(A, 0, true, s[2], rr_capture_stream(dev, 7)))) break;
         if ((rc = rr_handle(s[2], &hc))) break;
         { k_rr_decide<<<1, 32, 0, s[2]>>>(ctl, w.ctr, w.ctr + 16, hc, hc, 0); count_launch(); }
         { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[2]>>>(A.rec_, A.rec, A.tag, N,
@@ -1698,7 +1790,7 @@ static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *k
         l0 = g_launches.load();
         if ((rc = rr_cond(s[2], hc, cudaGraphCondTypeWhile, &body[3]))) break;
         if ((rc = begin(3))) break;
-        if ((rc = rr_iteration(A, 1, false, s[3]))) break;
+        if ((rc = rr_iteration(A, 1, false, s[3], rr_capture_stream(dev, 8)))) break;
         if ((rc = rr_handle(s[3], &hm))) break;
         { k_rr_decide<<<1, 32, 0, s[3]>>>(ctl, w.ctr, w.ctr, hc, hm, 1); count_launch(); }
         { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[3]>>>(A.rec_, A.rec, A.tag, N,
@@ -1706,7 +1798,7 @@ static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *k
         kc->it2 = g_launches.load() - l0;
         if ((rc = rr_cond(s[3], hm, cudaGraphCondTypeIf, &body[4]))) break;
         if ((rc = begin(4))) break;
-        if ((rc = rr_iteration(A, 0, false, s[4]))) break;
+        if ((rc = rr_iteration(A, 0, false, s[4], rr_capture_stream(dev, 9)))) break;
         { k_rr_decide<<<1, 32, 0, s[4]>>>(ctl, w.ctr, w.ctr + 16, hc, hc, 0); count_launch(); }
         { k_sync_tagged<<<div_up(div_up(N, 4), 256), 256, 0, s[4]>>>(A.rec_, A.rec, A.tag, N,
                                                                    ((uintptr_t)A.tag & 3) == 0, ctl + 4); count_launch(); }
@@ -1718,6 +1810,11 @@ static int rr_capture(const RRBufs &A, int dev, cudaGraph_t G, RRKernelCounts *k
         }
         if (rc) break;
         PFF_MODE_DISPATCH(g.mode, l_basin_init_if, A.bid, g, ctl + 5, s[0]);
+        if (ctl_out) {
+            l0 = g_launches.load();
+            { k_rr_ctl_copy<<<1, 32, 0, s[0]>>>(ctl, ctl_out); count_launch(); }
+            kc->tail = g_launches.load() - l0;
+        }
     } while (0);
     // end every capture still open (innermost first)
     for (int d = depth - 1; d >= 0; --d) {
@@ -1764,10 +1861,23 @@ static bool rr_graphs_on()
 // Launch the device-driven loop for these buffers (a graph built and kept on the
 // first call with them), then read its final state (one synchronisation).
 // Returns PFF_ERR_UNSUPPORTED when graphs cannot be built here.
+// Kernels one launch of a graph ran, from its final state words c[0..8].
+static long long rr_tally(const RRKernelCounts &kc, const int *c)
+{
+    long long nk = kc.pro + kc.tail;  // prologue, body A, iteration 0, then the iterations of the WHILE
+    if (c[6]) nk += kc.a;
+    if (c[7] && c[8] > 0) nk += kc.b0 + (long long)(c[8] - 1) * kc.it2;
+    return nk + (c[5] ? 1 : 0);  // + basin_id_init
+}
+
+// ctl_out: NULL, or a device buffer of 9 ints that the graph's last node fills with its
+// final state (a separate graph variant).  launch_only: return after the launch (the
+// caller reads the state later); kc_out receives the graph's kernel counts.
 static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z, float *z_prime,
                          uint8_t *is_border, long long *out, long long *sad, int32_t *snode, uint8_t *tag,
                          uint8_t *tag_, const Grid &g, RerouteWs &w, void *workspace, size_t workspace_bytes,
-                         int *state, int *it, int *outer, int *n_outer, cudaStream_t st)
+                         int *state, int *it, int *outer, int *n_outer, cudaStream_t st, int *ctl_out = nullptr,
+                         bool launch_only = false, RRKernelCounts *kc_out = nullptr)
 {
     static std::mutex mu;
     static RREntry cache[8];
@@ -1783,7 +1893,7 @@ static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec
     for (const void *p : {(const void *)bid, (const void *)rec, (const void *)rec_, (const void *)rec__,
                           (const void *)z, (const void *)z_prime, (const void *)is_border, (const void *)out,
                           (const void *)sad, (const void *)snode, (const void *)tag, (const void *)tag_,
-                          (const void *)g.codes, (const void *)w.inv, (const void *)w.ctr})
+                          (const void *)g.codes, (const void *)w.inv, (const void *)w.ctr, (const void *)ctl_out})
         key.add(p);
     key.add((unsigned long long)g.nx);
     key.add((unsigned long long)g.ny);
@@ -1799,7 +1909,7 @@ static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec
             cudaGraph_t G = nullptr;
             PFF_CUDA(cudaGraphCreate(&G, 0));
             const long long l0 = g_launches.load();
-            int rc = rr_capture(bufs, dev, G, &kc);
+            int rc = rr_capture(bufs, dev, G, &kc, ctl_out);
             g_launches.store(l0);  // captured, not launched: replays are counted below
             if (rc == PFF_OK && cudaGraphInstantiate(&exec, G, 0) != cudaSuccess) {
                 set_error("reroute graph: instantiate: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1820,17 +1930,15 @@ static int reroute_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec
         }
     }
     PFF_CUDA(cudaGraphLaunch(exec, st));
+    if (kc_out) *kc_out = kc;
+    if (launch_only) return check_cuda("reroute graph launch");
     int c[9];
     PFF_TRY(read_ints(IntReads().add(w.ctr + RR_CTL, 9), c, st));
     *it = c[0];
     *outer = c[1];
     *n_outer = c[2];
     *state = c[3];
-    // kernels this launch ran: prologue, body A, iteration 0, then the iterations of the WHILE
-    long long nk = kc.pro;
-    if (c[6]) nk += kc.a;
-    if (c[7] && c[8] > 0) nk += kc.b0 + (long long)(c[8] - 1) * kc.it2;
-    g_launches.fetch_add(nk + (c[5] ? 1 : 0));  // + basin_id_init
+    g_launches.fetch_add(rr_tally(kc, c));
     return check_cuda("reroute graph launch");
 }
 
@@ -1970,6 +2078,7 @@ static int reroute_host_loop(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t 
             coop_relabel = nsm * (per < 4 ? per : 4);
         }
         int *plist = w.pits[par];
+        { k_relabel_jump_block<<<1, 1024, 0, st>>>(w.fin, plist, np, cudaGraphConditionalHandle{}, 0); count_launch(); }
         void *args[] = {&w.fin, &plist, &np, &flags};
         PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, st));
         count_launch();
@@ -2002,7 +2111,7 @@ static int reroute_host_loop(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t 
             ++n_outer;  // the next iteration would count 0 pits, label, then break (:512-514)
             break;      // its labels are reset by basin_id_init (:537) anyway
         }
-        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, rec_, rec, tag, N,
+        { k_relabel<<<div_up(div_up(N, 4), B), B, 0, st>>>(bid, w.fin, rec_, rec, tag, tag_, N,
                                                            ((uintptr_t)bid & 15) == 0 && ((uintptr_t)tag & 3) == 0); count_launch(); }
         if (ndirty > 0)
             PFF_MODE_DISPATCH(g.mode, l_tile_terminal_list, rec_, rec__, w.R, w.ctr + 16 * par, g, w.tiles, w.ctr + 44,
@@ -2027,6 +2136,33 @@ static int reroute_host_loop(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t 
 }
 
 }  // namespace pff
+
+// What the host does after the device-driven loop stopped in `state` (iteration it,
+// bound outer, n_outer iterations counted): nothing for a finished loop, the
+// reference's steps on the host for the general cases, an error otherwise.
+static int reroute_after_graph(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
+                               float *z_prime, uint8_t *is_border, long long *out, long long *sad,
+                               int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, const Grid &g, RerouteWs &w,
+                               int state, int it, int outer, int n_outer, int *n_outer_out, cudaStream_t st)
+{
+    if (state == RR_NOPITS) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
+    if (state == RR_GENERAL)  // non-D4 receivers or a receiver cycle in the input: the reference's steps
+        return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag, tag_,
+                                 1, g, w, 0, 0, true, 0, n_outer_out, st);
+    if (state == RR_RESUME)  // the carve closed a receiver cycle: the reference's steps from here on
+        return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag, tag_,
+                                 1, g, w, it + 1, outer, true, n_outer, n_outer_out, st);
+    if (state == RR_WALKERR) {
+        set_error("pff_reroute_flow: carve walk exceeded its bounds");
+        return PFF_ERR_NOCONV;
+    }
+    if (state != RR_DONE) {
+        set_error("pff_reroute_flow: outer loop ended in state %d", state);
+        return PFF_ERR_NOCONV;
+    }
+    if (n_outer_out) *n_outer_out = n_outer;
+    return check_cuda("pff_reroute_flow");
+}
 
 extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z,
                                 float *z_prime, uint8_t *is_border, int64_t *outlet, int64_t *basin_saddle,
@@ -2056,25 +2192,9 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
         int state = 0, it = 0, outer = 0, n_outer = 0;
         const int rc = reroute_graph(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag,
                                      tag_, g, w, workspace, workspace_bytes, &state, &it, &outer, &n_outer, st);
-        if (rc == PFF_OK) {
-            if (state == RR_NOPITS) return check_cuda("pff_reroute_flow");  // :496-497, bid untouched
-            if (state == RR_GENERAL)  // non-D4 receivers or a receiver cycle in the input: the reference's steps
-                return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode,
-                                         tag, tag_, carve, g, w, 0, 0, true, 0, n_outer_out, st);
-            if (state == RR_RESUME)  // the carve closed a receiver cycle: the reference's steps from here on
-                return reroute_host_loop(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode,
-                                         tag, tag_, carve, g, w, it + 1, outer, true, n_outer, n_outer_out, st);
-            if (state == RR_WALKERR) {
-                set_error("pff_reroute_flow: carve walk exceeded its bounds");
-                return PFF_ERR_NOCONV;
-            }
-            if (state != RR_DONE) {
-                set_error("pff_reroute_flow: outer loop ended in state %d", state);
-                return PFF_ERR_NOCONV;
-            }
-            if (n_outer_out) *n_outer_out = n_outer;
-            return check_cuda("pff_reroute_flow");
-        }
+        if (rc == PFF_OK)
+            return reroute_after_graph(bid, rec, rec_, rec__, z, z_prime, is_border, out, sad, basin_saddlenode, tag,
+                                       tag_, g, w, state, it, outer, n_outer, n_outer_out, st);
         if (rc != PFF_ERR_UNSUPPORTED) return rc;
         clear_error();  // graphs unavailable: the host-driven loop below
     }
@@ -2092,4 +2212,251 @@ extern "C" int pff_reroute_use_graphs(int on)
     const int prev = rr_graphs_on() ? 1 : 0;
     g_rr_graphs.store(on != 0 ? 1 : 0);
     return prev;
+}
+
+// ---- asynchronous reroute ----------------------------------------------------------
+// pff_reroute_flow split at its one synchronisation: the graph launch, whose last node
+// copies the final state words into ctl_out, and the host's continuation from a host
+// copy of those words.
+
+#define PFF_REROUTE_ARGS                                                                                        \
+    int32_t *bid, int32_t *rec, int32_t *rec_, int32_t *rec__, const float *z, float *z_prime, uint8_t *is_border, \
+        int64_t *outlet, int64_t *basin_saddle, int32_t *basin_saddlenode, uint8_t *tag, uint8_t *tag_, int nx,  \
+        int ny, int bound_mode, const uint8_t *codes, void *workspace, size_t workspace_bytes
+
+static int reroute_args_ok(const char *who, PFF_REROUTE_ARGS)
+{
+    PFF_TRY(check_grid(nx, ny, bound_mode, codes));
+    if (!bid || !rec || !rec_ || !rec__ || !z || !z_prime || !is_border || !outlet || !basin_saddle ||
+        !basin_saddlenode || !tag || !tag_) {
+        set_error("%s: null pointer", who);
+        return PFF_ERR_ARG;
+    }
+    if (!workspace || workspace_bytes < pff_reroute_workspace_bytes(nx * ny)) {
+        set_error("%s: workspace too small", who);
+        return PFF_ERR_WORKSPACE;
+    }
+    return PFF_OK;
+}
+
+// kernel counts of the last asynchronous launch per device (for the launch tally)
+static RRKernelCounts g_async_kc[64];
+
+extern "C" int pff_reroute_flow_async(PFF_REROUTE_ARGS, int *ctl_out, void *stream)
+{
+    clear_error();
+    PFF_TRY(reroute_args_ok("pff_reroute_flow_async", bid, rec, rec_, rec__, z, z_prime, is_border, outlet,
+                            basin_saddle, basin_saddlenode, tag, tag_, nx, ny, bound_mode, codes, workspace,
+                            workspace_bytes));
+    if (!ctl_out) {
+        set_error("pff_reroute_flow_async: null ctl_out");
+        return PFF_ERR_ARG;
+    }
+    Grid g{nx, ny, bound_mode, codes};
+    RerouteWs w = carve_ws(workspace, workspace_bytes, nx * ny);
+    int dev = 0;
+    PFF_CUDA(cudaGetDevice(&dev));
+    int state = 0, it = 0, outer = 0, n_outer = 0;
+    RRKernelCounts kc{};
+    const int rc = reroute_graph(bid, rec, rec_, rec__, z, z_prime, is_border, (long long *)outlet,
+                                 (long long *)basin_saddle, basin_saddlenode, tag, tag_, g, w, workspace,
+                                 workspace_bytes, &state, &it, &outer, &n_outer, S(stream), ctl_out, true, &kc);
+    if (rc == PFF_ERR_UNSUPPORTED) {
+        set_error("pff_reroute_flow_async: the device-driven loop is not available (graphs switched off or "
+                  "not supported here); use pff_reroute_flow");
+        return PFF_ERR_UNAVAILABLE;
+    }
+    PFF_TRY(rc);
+    if (dev >= 0 && dev < 64) g_async_kc[dev] = kc;
+    return PFF_OK;
+}
+
+extern "C" int pff_reroute_flow_finish(PFF_REROUTE_ARGS, const int *ctl_host, int *n_outer_out, void *stream)
+{
+    clear_error();
+    PFF_TRY(reroute_args_ok("pff_reroute_flow_finish", bid, rec, rec_, rec__, z, z_prime, is_border, outlet,
+                            basin_saddle, basin_saddlenode, tag, tag_, nx, ny, bound_mode, codes, workspace,
+                            workspace_bytes));
+    if (!ctl_host) {
+        set_error("pff_reroute_flow_finish: null ctl_host");
+        return PFF_ERR_ARG;
+    }
+    if (n_outer_out) *n_outer_out = 0;
+    int dev = 0;
+    PFF_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64) g_launches.fetch_add(rr_tally(g_async_kc[dev], ctl_host));
+    Grid g{nx, ny, bound_mode, codes};
+    RerouteWs w = carve_ws(workspace, workspace_bytes, nx * ny);
+    return reroute_after_graph(bid, rec, rec_, rec__, z, z_prime, is_border, (long long *)outlet,
+                               (long long *)basin_saddle, basin_saddlenode, tag, tag_, g, w, ctl_host[3], ctl_host[0],
+                               ctl_host[1], ctl_host[2], n_outer_out, S(stream));
+}
+
+// ---- a region that runs only after a finished reroute ------------------------------------
+// A graph: k_guard_set, then an IF node whose body is whatever the caller issues on
+// its stream between pff_guard_begin and pff_guard_end.  The body runs when the
+// reroute state in ctl[3] is "finished" (no pits, or done on the device) and the
+// caller's flag (if any) is zero.
+
+__global__ void k_guard_set(const int *ctl, const int *flag, cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x) return;
+    const int st = ctl[3];
+    const bool go = (st == RR_NOPITS || st == RR_DONE) && (!flag || *flag == 0);
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+namespace {
+struct Guard {
+    cudaGraph_t G = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capturing = nullptr;
+    bool used = false;
+};
+constexpr int GUARDS = 1024;
+std::mutex g_guard_mu;
+Guard g_guards[GUARDS];
+}  // namespace
+
+extern "C" int pff_guard_begin(const int *ctl, const int *flag, void *stream, int *id)
+{
+    clear_error();
+    if (!ctl || !id || !stream) {
+        set_error("pff_guard_begin: bad arguments (a non-default stream is required)");
+        return PFF_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_guard_mu);
+    int k = 0;
+    while (k < GUARDS && g_guards[k].used) ++k;
+    if (k == GUARDS) {
+        set_error("pff_guard_begin: too many guarded regions");
+        return PFF_ERR_ARG;
+    }
+    Guard &gd = g_guards[k];
+    PFF_CUDA(cudaGraphCreate(&gd.G, 0));
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, gd.G, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cudaGraphDestroy(gd.G);
+        gd.G = nullptr;
+        return check_cuda("pff_guard_begin: conditional handle");
+    }
+    cudaKernelNodeParams kp{};
+    void *args[] = {(void *)&ctl, (void *)&flag, (void *)&h};
+    kp.func = (void *)k_guard_set;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = args;
+    cudaGraphNode_t kn, cn;
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    if (cudaGraphAddKernelNode(&kn, gd.G, nullptr, 0, &kp) != cudaSuccess ||
+        cudaGraphAddNode(&cn, gd.G, &kn, 1, &cp) != cudaSuccess ||
+        cudaStreamBeginCaptureToGraph(S(stream), cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGraphDestroy(gd.G);
+        gd.G = nullptr;
+        return check_cuda("pff_guard_begin");
+    }
+    gd.capturing = S(stream);
+    gd.used = true;
+    *id = k;
+    return PFF_OK;
+}
+
+extern "C" int pff_guard_end(int id, void *stream)
+{
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_guard_mu);
+    if (id < 0 || id >= GUARDS || !g_guards[id].used || !g_guards[id].G || g_guards[id].capturing != S(stream)) {
+        set_error("pff_guard_end: no region %d open on this stream", id);
+        return PFF_ERR_ARG;
+    }
+    Guard &gd = g_guards[id];
+    cudaGraph_t body = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(gd.capturing, &body);
+    gd.capturing = nullptr;
+    if (e == cudaSuccess && cudaGraphInstantiate(&gd.exec, gd.G, 0) == cudaSuccess) return PFF_OK;
+    set_error("pff_guard_end: %s", cudaGetErrorString(e != cudaSuccess ? e : cudaGetLastError()));
+    cudaGetLastError();
+    cudaGraphDestroy(gd.G);
+    gd = Guard{};
+    return PFF_ERR_CUDA;
+}
+
+extern "C" int pff_guard_launch(int id, void *stream)
+{
+    clear_error();
+    cudaGraphExec_t exec = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_guard_mu);
+        if (id >= 0 && id < GUARDS && g_guards[id].used) exec = g_guards[id].exec;
+    }
+    if (!exec) {
+        set_error("pff_guard_launch: region %d is not complete", id);
+        return PFF_ERR_ARG;
+    }
+    PFF_CUDA(cudaGraphLaunch(exec, S(stream)));
+    return PFF_OK;
+}
+
+extern "C" int pff_guard_destroy(int id)
+{
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_guard_mu);
+    if (id < 0 || id >= GUARDS || !g_guards[id].used) {
+        set_error("pff_guard_destroy: no region %d", id);
+        return PFF_ERR_ARG;
+    }
+    Guard &gd = g_guards[id];
+    if (gd.capturing) {
+        cudaGraph_t body = nullptr;
+        cudaStreamEndCapture(gd.capturing, &body);
+    }
+    if (gd.exec) cudaGraphExecDestroy(gd.exec);
+    if (gd.G) cudaGraphDestroy(gd.G);
+    gd = Guard{};
+    cudaGetLastError();
+    return PFF_OK;
+}
+
+// flag[0] = 1 if (double)val[0] / div < thr, else 0: the host's residual test
+// (float(value) / dt < threshold, in double) made on the device
+__global__ void k_residual_flag(const float *val, double div, double thr, int *flag)
+{
+    if (threadIdx.x == 0) flag[0] = ((double)val[0] / div < thr) ? 1 : 0;
+}
+
+// out_dev[0] (if given) and out_host[0] (pinned host memory, written through its
+// unified address; if given) = val[0]: one kernel instead of two copies
+__global__ void k_value_store(const float *val, float *out_dev, float *out_host)
+{
+    if (threadIdx.x) return;
+    const float v = val[0];
+    if (out_dev) out_dev[0] = v;
+    if (out_host) *(volatile float *)out_host = v;
+}
+
+extern "C" int pff_value_store(const float *val, float *out_dev, float *out_host, void *stream)
+{
+    clear_error();
+    if (!val) {
+        set_error("pff_value_store: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    { k_value_store<<<1, 32, 0, S(stream)>>>(val, out_dev, out_host); count_launch(); }
+    return check_cuda("pff_value_store");
+}
+
+extern "C" int pff_residual_flag(const float *val, double div, double thr, int *flag, void *stream)
+{
+    clear_error();
+    if (!val || !flag) {
+        set_error("pff_residual_flag: bad arguments");
+        return PFF_ERR_ARG;
+    }
+    { k_residual_flag<<<1, 32, 0, S(stream)>>>(val, div, thr, flag); count_launch(); }
+    return check_cuda("pff_residual_flag");
 }

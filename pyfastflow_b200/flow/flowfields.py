@@ -28,7 +28,7 @@ class FlowRouter:
         self.mode = cte.BOUND_MODES[boundary_mode]
         self.lakeflow = lakeflow
         self.stochastic_receivers = bool(stochastic_receivers)
-        self.device = torch.device(device)
+        self.device = _dev.resolve_device(device)
         N = self.nx * self.ny
         self.N = N
         f32, i32 = dict(dtype=torch.float32, device=self.device), dict(dtype=torch.int32, device=self.device)
@@ -143,6 +143,44 @@ class FlowRouter:
                   self.tag.data_ptr(), self.tag_.data_ptr(), int(bool(carve)), self.nx, self.ny, self.mode,
                   self._codes(), wp, wn, C.byref(nout), _dev.stream())
         self.last_n_outer = nout.value
+
+    def _reroute_args(self):
+        n = self.N
+        wp, wn = self._ws_lake.get(_lib.load().pff_reroute_workspace_bytes(n), self.device)
+        return (self.bid.data_ptr(), self.receivers.data_ptr(), self.receivers_.data_ptr(),
+                self.receivers__.data_ptr(), self.z.data_ptr(), self.z_.data_ptr(), self.is_border.data_ptr(),
+                self.outlet.data_ptr(), self.basin_saddle.data_ptr(), self.basin_saddlenode.data_ptr(),
+                self.tag.data_ptr(), self.tag_.data_ptr(), self.nx, self.ny, self.mode, self._codes(), wp, wn)
+
+    def reroute_flow_async(self, ctl: torch.Tensor) -> bool:
+        """Launch the carve reroute's device-driven loop without waiting for it; its
+        final state (9 int32) lands in `ctl` (a device tensor).  False where that
+        loop is not available (graphs switched off): call reroute_flow instead.
+        Complete with reroute_flow_finish once a host copy of `ctl` is readable."""
+        if not self.lakeflow:
+            raise RuntimeError("Flow field not compiled for lakeflow")
+        lib = _lib.load()
+        _lib._sync_device()
+        rc = lib.pff_reroute_flow_async(*self._reroute_args(), ctl.data_ptr(), _dev.stream())
+        if rc == 5:  # PFF_ERR_UNAVAILABLE
+            return False
+        if rc != 0:
+            raise _lib.PFFError(f"pff_reroute_flow_async failed with status {rc}: "
+                                f"{lib.pff_last_error_string().decode(errors='replace')}")
+        return True
+
+    def reroute_flow_finish(self, ctl_host) -> int:
+        """The host's part of an asynchronous reroute, from a host copy of its state
+        (pinned int32 tensor of 9): nothing if the loop finished on the device, the
+        reference's steps on the host if it stopped for them.  Returns the reroute's
+        state word (1 no pits, 2 done on the device, 3-4 finished on the host)."""
+        import ctypes as C
+
+        nout = C.c_int()
+        _lib.call("pff_reroute_flow_finish", *self._reroute_args(), ctl_host.data_ptr(), C.byref(nout),
+                  _dev.stream())
+        self.last_n_outer = nout.value
+        return int(ctl_host[3])
 
     def _accumulate(self, counts: bool = True, exact_order: bool = False, value=None):
         """Upstream sums of the seeds (Q, or `value` per cell) into Q and counts.

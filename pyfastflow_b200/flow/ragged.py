@@ -65,7 +65,7 @@ class RaggedRouter:
         self.ntiles = len(shapes)
         if self.ntiles == 0:
             raise ValueError("empty batch")
-        self.device = torch.device(device or "cuda")
+        self.device = _dev.resolve_device(device or "cuda")
         self.ny = np.array([int(s[0]) for s in shapes], np.int32)
         self.nx = np.array([int(s[1]) for s in shapes], np.int32)
         dxs = np.broadcast_to(np.asarray(dx, np.float64), (self.ntiles,))

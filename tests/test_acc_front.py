@@ -44,8 +44,9 @@ def _run(torch, rcv, w, nx, ny, mode, front):
     cd = torch.zeros(N, dtype=torch.int32, device="cuda")
     ws = torch.empty(lib.pff_accumulate_workspace_bytes(N), dtype=torch.uint8, device="cuda")
     assert lib.pff_accumulate_set_front(front) == 0
+    rd = torch.from_numpy(rcv).cuda()  # held until the kernels have run
     try:
-        _lib.call("pff_accumulate_grid", torch.from_numpy(rcv).cuda().data_ptr(), Qd.data_ptr(), cd.data_ptr(), nx,
+        _lib.call("pff_accumulate_grid", rd.data_ptr(), Qd.data_ptr(), cd.data_ptr(), nx,
                   ny, mode, None, N, ws.data_ptr(), ws.numel(), _dev.stream())
     finally:
         lib.pff_accumulate_set_front(DEFAULT)

@@ -157,6 +157,37 @@ def test_manning_core(orc, cuda):
     assert np.isnan(host(hd)[::17]).all()
 
 
+def test_manning_core_one_pass(orc, cuda):
+    """pff_graphflood_core_filled (slopes from a copy of zh, both loops in one pass)
+    equals the two-loop update and the oracle bit for bit, residual included."""
+    torch = cuda
+    from pyfastflow_b200 import _dev, _lib
+
+    og, zh, h, rcv = state(orc, 160, 96, 1, 17, h_scale=0.3)
+    rng = np.random.default_rng(4)
+    Q = (rng.random(og.N) * 40).astype(np.float32)
+    h[::13] = -0.02
+    h[5::29] = 0.0
+    args = (og.N, 10.0, 100.0, 0.033, 1e-2, 5e-3)  # rounded to f32 by the binding
+    out = {}
+    rd, qd = dev(torch, rcv), dev(torch, Q)  # held: a freed temporary's block could be reused by the next
+    for fn in ("pff_graphflood_core", "pff_graphflood_core_filled"):
+        hd, zd, zf = dev(torch, h), dev(torch, zh), dev(torch, zh)
+        dh = torch.zeros(og.N, dtype=torch.float32, device="cuda")
+        href = dev(torch, h + 0.01)
+        dmax = torch.zeros(1, dtype=torch.float32, device="cuda")
+        ptrs = [hd.data_ptr(), zd.data_ptr()] + ([zf.data_ptr()] if fn.endswith("filled") else [])
+        _lib.call(fn, *ptrs, dh.data_ptr(), rd.data_ptr(), qd.data_ptr(), *args, href.data_ptr(), dmax.data_ptr(),
+                  _dev.stream())
+        out[fn] = [host(hd), host(zd), host(dh), host(dmax)]
+    ho, zo, dho = orc.graphflood_core(h.copy(), zh.copy(), rcv, Q, 10.0, 0.033, 1e-2, 5e-3)
+    for a, b in zip(out["pff_graphflood_core"], out["pff_graphflood_core_filled"]):
+        assert np.array_equal(bits(a), bits(b))
+    got = out["pff_graphflood_core_filled"]
+    assert np.array_equal(bits(got[0]), bits(ho)) and np.array_equal(bits(got[1]), bits(zo))
+    assert np.array_equal(bits(got[2]), bits(dho))
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_flooder_iterations(orc, cuda, mode):
     """Flooder.run_graphflood vs the oracle's run of the same iterations."""
@@ -176,6 +207,90 @@ def test_flooder_iterations(orc, cuda, mode):
     assert np.array_equal(bits(fl.get_h().ravel()), bits(h))
     assert np.array_equal(bits(router.get_Z().ravel()), bits(zh))
     assert np.array_equal(bits(router.get_Q().ravel()), bits(Q))
+
+
+@pytest.mark.parametrize("stop", ["max", "mean"])
+def test_run_to_residual_stops_at_the_first_converged_iteration(cuda, stop):
+    """run_to_residual reads each residual one iteration late (at the next reroute's
+    synchronisation); it must still stop at the first iteration whose residual is
+    below the threshold, with h, z and Q of that iteration, and report the same
+    residual trace as a plain loop that checks after every iteration."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+    from pyfastflow_b200 import constants as cte
+
+    nx, ny, dx, P = 128, 96, 10.0, 1e-5
+    z = synthetic.spectral_dem(nx, ny, 21, relief=40.0, npits=8, pit_scale=0.2)
+
+    def fresh():
+        router = pf.flow.FlowRouter(nx, ny, dx)
+        router.set_z(z)
+        return router, pf.graphflood.Flooder(router, precipitation_rates=P, manning=0.033, edge_slope=1e-2)
+
+    router, fl = fresh()
+    res = []
+    for _ in range(40):
+        h0 = fl.h.clone()
+        fl.iteration()
+        d = (fl.h - h0).abs()
+        res.append(float(d.max() if stop == "max" else d.float().mean()) / cte.DT_HYDRO)
+    srt = sorted(res)  # a threshold halfway between two residuals from the middle of the run
+    thr = 0.5 * (srt[len(srt) // 2] + srt[len(srt) // 2 + 1])
+    first = next(k for k, r in enumerate(res) if r < thr) + 1
+    r2, fl2 = fresh()
+    for _ in range(first):
+        fl2.iteration()
+    torch.cuda.synchronize()
+    # the pipelined loop (guarded post-reroute graphs), and the one-by-one loop it
+    # falls back to where the device-driven reroute is switched off
+    from pyfastflow_b200 import _lib
+
+    for graphs in (1, 0):
+        prev = _lib.load().pff_reroute_use_graphs(graphs)
+        try:
+            router, fl = fresh()
+            n, why, r = fl.run_to_residual(tol_ratio=thr / P, max_iter=40, return_trace=False, stop=stop)
+        finally:
+            _lib.load().pff_reroute_use_graphs(prev)
+        torch.cuda.synchronize()
+        assert n == first and why == "residual", graphs
+        assert r == pytest.approx(res[first - 1], rel=1e-5)
+        assert torch.equal(fl.h, fl2.h) and torch.equal(router.z, r2.z) and torch.equal(router.Q, r2.Q)
+    # the cap: max_iter iterations, the last residual reported
+    router, fl = fresh()
+    n, why, r, tr = fl.run_to_residual(tol_ratio=1e-30, max_iter=7, return_trace=True, stop=stop)
+    assert n == 7 and why == "max_iter" and len(tr) == 7
+    assert np.allclose(tr, res[:7], rtol=1e-5) and r == pytest.approx(res[6], rel=1e-5)
+
+
+def test_pipelined_run_equals_iterations(cuda):
+    """run_graphflood's pipelined loop (asynchronous reroute, guarded post-reroute
+    graph) leaves h, z, Q and the router's fields exactly as the same number of
+    single iterations does, periodic boundaries included, also when the two loops
+    alternate on one Flooder (a workspace reallocated under a captured graph once
+    made that fault)."""
+    torch = cuda
+    import pyfastflow_b200 as pf
+
+    nx, ny = 192, 160
+    z = synthetic.spectral_dem(nx, ny, 8, relief=80.0, npits=30, pit_scale=0.3)
+    outs = []
+    for pipelined in (True, False):
+        router = pf.flow.FlowRouter(nx, ny, 10.0, boundary_mode="periodic_EW")
+        router.set_z(z)
+        fl = pf.graphflood.Flooder(router, precipitation_rates=2e-5, manning=0.04, edge_slope=1e-2)
+        if pipelined:  # both loops on one Flooder: their graphs share its workspaces
+            fl.run_graphflood(10)
+            for _ in range(5):
+                fl.iteration()
+            fl.run_graphflood(10)
+        else:
+            for _ in range(25):
+                fl.iteration()
+        torch.cuda.synchronize()
+        outs.append([t.clone() for t in (fl.h, router.z, router.Q, router.receivers, router.bid, router.z_)])
+    for a, b in zip(*outs):  # bit patterns: NaN depths compare equal too
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32))
 
 
 @pytest.mark.gpu

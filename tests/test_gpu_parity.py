@@ -171,8 +171,9 @@ def test_reroute(orc, cuda, mode, carve):
     torch = cuda
     from pyfastflow_b200 import flow
 
+    # uniform 400 x 300: about 24,000 pits, more than one CTA's basin relabelling takes
     for kind, (nx, ny) in [("spectral", (211, 173)), ("int", (64, 48)), ("int", (9, 7)), ("uniform", (130, 66)),
-                           ("spectral", (512, 384))]:
+                           ("spectral", (512, 384)), ("uniform", (400, 300))]:
         g = Grid(orc, torch, nx, ny, mode, seed=7)
         z = make_case(kind, nx, ny, seed=31 + mode)
         set_constants(g, 10.0)
@@ -320,12 +321,12 @@ def test_accumulate_general_forest(orc, cuda, grid_given):
         Qd = dev(torch, w)
         cd = torch.zeros(N, dtype=torch.int32, device="cuda")
         wp, wn = ws.get(_lib.load().pff_accumulate_workspace_bytes(N))
+        rd = dev(torch, rcv)  # held until the kernels have run
         if grid_given:
-            _lib.call("pff_accumulate_grid", dev(torch, rcv).data_ptr(), Qd.data_ptr(), cd.data_ptr(), nx, ny, 0,
+            _lib.call("pff_accumulate_grid", rd.data_ptr(), Qd.data_ptr(), cd.data_ptr(), nx, ny, 0,
                       None, N, wp, wn, _dev.stream())
         else:
-            _lib.call("pff_accumulate", dev(torch, rcv).data_ptr(), Qd.data_ptr(), cd.data_ptr(), N, wp, wn,
-                      _dev.stream())
+            _lib.call("pff_accumulate", rd.data_ptr(), Qd.data_ptr(), cd.data_ptr(), N, wp, wn, _dev.stream())
         Qo, co = orc.accumulate(rcv, w)
         assert np.array_equal(host(cd).view(np.uint32), co)
         assert np.array_equal(host(Qd).view(np.uint32), Qo.view(np.uint32))

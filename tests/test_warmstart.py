@@ -81,7 +81,8 @@ def test_conv_channel_slices(cuda):
     ref = F.conv2d(xw[:, 8:24], w, padding=1)
     xd = _nhwc(xw).to(torch.bfloat16).cuda()
     y = torch.full((B * H * W * 48,), 7.0, dtype=torch.float32, device="cuda")
-    _lib.call("pff_conv3x3_fwd", xd.data_ptr(), 32, 8, _w_ours(w).to(torch.bfloat16).cuda().data_ptr(), None,
+    wd = _w_ours(w).to(torch.bfloat16).cuda()
+    _lib.call("pff_conv3x3_fwd", xd.data_ptr(), 32, 8, wd.data_ptr(), None,
               y.data_ptr(), 48, 16, B, H, W, Cin, Cout, 0, 1, _dev.stream())
     yy = _nchw(y.cpu(), B, H, W, 48)
     assert _rel(yy[:, 16:40], ref) < 1e-4
@@ -136,8 +137,8 @@ def test_pool_upsample_relu(cuda):
     # pooling backward adds into a slice of wider rows
     dy = _bf(torch.randn(B, C, H // 2, W // 2, generator=g))
     base = torch.ones(B * H * W * 2 * C, dtype=torch.bfloat16, device="cuda")
-    _lib.call("pff_avgpool2_bwd", _nhwc(dy).to(torch.bfloat16).cuda().data_ptr(), C, 0, base.data_ptr(), 2 * C, C, B,
-              H, W, C, 1, st)
+    dyd = _nhwc(dy).to(torch.bfloat16).cuda()
+    _lib.call("pff_avgpool2_bwd", dyd.data_ptr(), C, 0, base.data_ptr(), 2 * C, C, B, H, W, C, 1, st)
     got = _nchw(base.float().cpu(), B, H, W, 2 * C)
     ref = 1 + F.interpolate(dy, scale_factor=2, mode="nearest") / 4
     assert _rel(got[:, C:], ref) < 1e-2 and (got[:, :C] == 1).all()
@@ -148,8 +149,8 @@ def test_pool_upsample_relu(cuda):
                        F.interpolate(x, scale_factor=2, mode="nearest"))
     du = _bf(torch.randn(B, 2 * C, 2 * H, 2 * W, generator=g))
     dxu = torch.zeros(B * H * W * C, dtype=torch.bfloat16, device="cuda")
-    _lib.call("pff_upsample2_bwd", _nhwc(du).to(torch.bfloat16).cuda().data_ptr(), 2 * C, 0, dxu.data_ptr(), C, 0, B,
-              H, W, C, st)
+    dud = _nhwc(du).to(torch.bfloat16).cuda()
+    _lib.call("pff_upsample2_bwd", dud.data_ptr(), 2 * C, 0, dxu.data_ptr(), C, 0, B, H, W, C, st)
     assert _rel(_nchw(dxu.float().cpu(), B, H, W, C), F.avg_pool2d(du[:, :C], 2) * 4) < 1e-2
     # ReLU backward: zero where the output is not positive
     gr = torch.ones(B * H * W * C, dtype=torch.bfloat16, device="cuda")
@@ -166,8 +167,9 @@ def test_adam_matches_formula(cuda):
     p0, gr = torch.randn(n, generator=g), torch.randn(n, generator=g)
     p, m, v = p0.clone().cuda(), torch.zeros(n).cuda(), torch.zeros(n).cuda()
     pb = torch.zeros(n, dtype=torch.bfloat16, device="cuda")
+    grd = gr.cuda()
     for step in (1, 2):
-        _lib.call("pff_adam", p.data_ptr(), gr.cuda().data_ptr(), m.data_ptr(), v.data_ptr(), pb.data_ptr(), n, 1e-2,
+        _lib.call("pff_adam", p.data_ptr(), grd.data_ptr(), m.data_ptr(), v.data_ptr(), pb.data_ptr(), n, 1e-2,
                   0.9, 0.999, 1e-8, step, 0.0, _dev.stream())
     opt = torch.optim.Adam([p0.requires_grad_(True)], lr=1e-2)
     for _ in range(2):
@@ -234,6 +236,91 @@ def test_unet_gradients_vs_torch(cuda):
         cos = float(torch.dot(gw, rw) / (gw.norm() * rw.norm() + 1e-30))
         assert cos > 0.97, f"{name}: cosine {cos:.4f}"
         assert abs(float(gw.norm() / rw.norm()) - 1) < 0.05, name
+
+
+class _RoundBF16(torch.autograd.Function):
+    """Identity that rounds to bf16 both ways: where the GPU network stores an
+    activation (forward) and that activation's gradient (backward) in bf16."""
+
+    @staticmethod
+    def forward(ctx, t):
+        return _bf(t)
+
+    @staticmethod
+    def backward(ctx, g):
+        return _bf(g)
+
+
+def _torch_unet_bf16(net, x):
+    """_torch_unet with the GPU's storage rounding: every convolution output (after
+    bias and ReLU, except the f32 head) and every pooled tensor is rounded to bf16,
+    and so is the gradient flowing back into each of them."""
+    from pyfastflow_b200.warmstart.unet import LAYERS
+
+    p = net.p.cpu()
+    Ws, bs = {}, {}
+    for name, _, _, _, _, cin, cout, _, _ in LAYERS:
+        wo, nw, bo, _ = net.layers[name]
+        Ws[name] = _bf(p[wo:wo + nw]).reshape(cout, 3, 3, cin).permute(0, 3, 1, 2).clone().requires_grad_(True)
+        bs[name] = p[bo:bo + cout].clone().requires_grad_(True)
+    R = _RoundBF16.apply
+    c = lambda n, t: R(F.conv2d(t, Ws[n], bs[n], padding=1).clamp_min(0))  # noqa: E731
+    pool = lambda t: R(F.avg_pool2d(t, 2))  # noqa: E731
+    up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")  # noqa: E731
+    e0 = c("enc0b", c("enc0a", x))
+    e1 = c("enc1b", c("enc1a", pool(e0)))
+    e2 = c("enc2b", c("enc2a", pool(e1)))
+    e3 = c("botb", c("bota", pool(e2)))
+    d2 = c("dec2b", c("dec2a", torch.cat([up(e3), e2], 1)))
+    d1 = c("dec1b", c("dec1a", torch.cat([up(d2), e1], 1)))
+    d0 = c("dec0b", c("dec0a", torch.cat([up(d1), e0], 1)))
+    return F.conv2d(d0, Ws["head"], bs["head"], padding=1), Ws, bs
+
+
+@pytest.mark.gpu
+def test_unet_gradients_vs_bf16_storage_reference(cuda):
+    """The same comparison against a CPU network that rounds what the GPU stores in
+    bf16 (activations forward, activation gradients backward): what remains is f32
+    summation order and where a sum of two gradient paths is rounded, so the
+    prediction, the loss and every layer's weight and bias gradients agree tightly."""
+    from pyfastflow_b200.warmstart import UNet
+
+    B, H, W = 2, 16, 24
+    net = UNet(seed=1)
+    net.set_head_bias(0.0)
+    g = torch.Generator().manual_seed(11)
+    x = _bf(torch.randn(B, 8, H, W, generator=g) * 0.5)
+    x[:, 6:] = 0
+    tgt = torch.randn(B * H * W, generator=g)
+    pred = net.forward(_nhwc(x).to(torch.bfloat16).cuda(), B, H, W)
+    loss, dp = net.loss_grad(tgt.cuda())
+    net.backward(dp)
+    torch.cuda.synchronize()
+    ref, Ws, bs = _torch_unet_bf16(net, x)
+    pr = ref.permute(0, 2, 3, 1).reshape(-1, 8)[:, 0]
+    ours = pred.cpu().reshape(-1, 8)[:, 0]
+    rel_pred = _rel(ours, pr)
+    lref = ((pr - tgt) ** 2).mean()
+    rel_loss = abs(float(loss) - float(lref)) / float(lref)
+    # d loss / d pred is stored in bf16 on the GPU
+    dpr = _bf(torch.autograd.grad(lref, pr, retain_graph=True)[0])
+    pr.backward(dpr)
+    gpu_g = net.g.cpu()
+    worst_cos, worst_ratio, worst_b = 1.0, 0.0, 0.0
+    for name in Ws:
+        wo, nw, bo, cout = net.layers[name]
+        gw, rw = gpu_g[wo:wo + nw], _w_ours(Ws[name].grad)
+        gb, rb = gpu_g[bo:bo + cout], bs[name].grad
+        cos = float(torch.dot(gw, rw) / (gw.norm() * rw.norm() + 1e-30))
+        worst_cos = min(worst_cos, cos)
+        worst_ratio = max(worst_ratio, abs(float(gw.norm() / rw.norm()) - 1))
+        worst_b = max(worst_b, float((gb - rb).norm() / (rb.norm() + 1e-30)))
+    print(f"pred rel {rel_pred:.3e} loss rel {rel_loss:.3e} min cos {worst_cos:.6f} "
+          f"max |norm ratio - 1| {worst_ratio:.3e} max bias rel {worst_b:.3e}")
+    # measured on B200: pred 3.4e-3, loss 5.5e-7, cosine 0.9979, norm ratio 6.3e-3, bias 0.066
+    # (the bias gradient of a layer is a sum over pixels with cancellation); about 2x margin
+    assert rel_pred < 1e-2 and rel_loss < 1e-4
+    assert worst_cos > 0.995 and worst_ratio < 0.015 and worst_b < 0.15
 
 
 @pytest.mark.gpu

@@ -44,7 +44,7 @@ ALG_BYTES = {"receivers": 12, "reroute": 16, "accumulate": 16}
 # (None: the launch covers a varying list of tiles), and DRAM read + write bytes
 # of one 4096^2 launch from an ncu capture of this workload (None: not captured).
 KERNELS = {
-    "k_receivers": (12, 146.0e6),           # z in; receivers + gradient out
+    "k_receivers": (12, 152.3e6),           # z in; receivers + gradient out
     "k_tile_terminal<grid>": (8, None),     # receivers in; tile terminals out
     "k_tile_terminal<list>": (None, None),  # the tiles a carve changed
     "k_tree_tile<up>": (8, 251.0e6),        # receivers + seeds in
@@ -365,7 +365,7 @@ def main():
                             "unit": "GB/s", "frac": kr["frac"], "peak_source": pk_kind,
                             "alg_bytes_per_launch": kr["alg_bytes_per_launch"], "ms_per_launch": kr["ms_per_launch"],
                             "traffic": kr["traffic"],
-                            "traffic_note": "DRAM read+write of one 4096^2 launch from an ncu capture (67 + 79 MB), "
+                            "traffic_note": "DRAM read+write of one 4096^2 launch from an ncu capture (71.3 + 81.0 MB), "
                                             "scaled by cells"}
 
     # ---- e2e through the public API with host buffers ----
@@ -859,9 +859,61 @@ def graphflood_main(args):
            "h_stats": {"max": float(np.nanmax(h)), "mean": float(np.nanmean(h)), "nan": int(np.isnan(h).sum()),
                        "wet_cells_1cm": int((h > 0.01).sum())},
            "clocks": clk.summary()}
+    out["kernels"] = graphflood_kernel_probe(router, fl, reset, n, iters=min(20, args.max_iter))
     if args.fp64_iters > 0:
         out["fp64_check"] = graphflood_fp64_check(args.fp64_size, args.fp64_iters)
     print(json.dumps(out))
+
+
+# Probed kernels of a GraphFlood iteration: algorithmic bytes per cell of one launch
+# over the whole grid (None: the launch covers a varying list of tiles).
+GF_KERNELS = {
+    "k_receivers": 12,            # zh in; receivers + gradient out
+    "k_tile_terminal<grid>": 8,   # receivers in; tile terminals out
+    "k_tile_terminal<list>": None,
+    "k_fill_round_packed": 16,    # one 8-byte {pointer, z} record in and out per round (the gather at the pointer is extra)
+    "k_fill_round_late": 16,      # the same rounds from the tenth on (a round after a settled one returns at once)
+    "k_diffuse_fused": 12,        # zh + Q in; Q after all sweeps out
+    "k_core_fused": 28,           # receivers, filled z, h, Q in; dh, h, zh out
+}
+
+
+def graphflood_kernel_probe(router, fl, reset, n, iters):
+    """Per-kernel device times of `iters` GraphFlood iterations from the library's
+    event probes, run eagerly (no graphs: probes skip captured launches), with the
+    achieved algorithmic GB/s against the measured HBM copy bandwidth."""
+    import ctypes
+
+    import torch
+
+    from pyfastflow_b200 import _lib
+
+    lib = _lib.load()
+    pk, pk_kind = peak_hbm()
+    reset()
+    torch.cuda.synchronize()
+    prev_graphs, prev_fl = lib.pff_reroute_use_graphs(0), fl.graphs
+    fl.graphs = False
+    lib.pff_probe_enable(1)
+    for _ in range(iters):
+        fl.iteration()
+    torch.cuda.synchronize()
+    res = {"iterations": iters, "peak": pk, "peak_source": pk_kind, "unit": "GB/s"}
+    for name, bpc in GF_KERNELS.items():
+        tot, nl = ctypes.c_double(), ctypes.c_int()
+        if lib.pff_probe_read(name.encode(), ctypes.byref(tot), ctypes.byref(nl)) != 0 or nl.value == 0:
+            continue
+        per = tot.value / nl.value
+        k = {"ms_per_launch": per, "launches_per_iteration": nl.value / iters, "ms_per_iteration": tot.value / iters}
+        if bpc is not None:
+            k["alg_bytes_per_launch"] = bpc * n * n
+            k["achieved_gbs"] = bpc * n * n / (per * 1e-3) / 1e9
+            k["frac"] = k["achieved_gbs"] / pk
+        res[name] = k
+    lib.pff_probe_enable(0)
+    lib.pff_reroute_use_graphs(prev_graphs)
+    fl.graphs = prev_fl
+    return res
 
 
 def graphflood_fp64_check(n, iters):

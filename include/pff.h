@@ -82,6 +82,18 @@ int pff_compute_receivers_stochastic(const float *z, int32_t *receivers, float *
                                      float dx, int bound_mode, const uint8_t *codes,
                                      unsigned long long seed, void *stream);
 
+/* Which kernel pff_compute_receivers uses in modes 0-2 when nx % 4 == 0 and the
+ * arrays are 16-byte aligned: 1 (default) the lean kernel (one Markstein-corrected
+ * quotient per cell, drops shared between neighbours, edges on the same path) at
+ * 7 CTAs per SM, 2 the same at 8 CTAs per SM, 0 the earlier 4-column row walk.
+ * Results are identical.  Returns the previous setting.  No reference counterpart.
+ * pff_receivers_div_selfcheck: runs the lean kernel's quotient for cell size dx on
+ * every float in its exact range and counts the results that differ from the IEEE
+ * division (must be 0); *checked = how many floats were run.  Synchronous; a
+ * self-test, no reference counterpart. */
+int pff_receivers_set_path(int lean);
+int pff_receivers_div_selfcheck(float dx, long long *mismatches, long long *checked);
+
 /* ---- accumulation (rake and compress) ----------------------------------------
  * Kernel-level mirrors of pyfastflow/flow/downstream_propag.py with identical
  * semantics (donor slots in ascending donor index, as the reference's serial

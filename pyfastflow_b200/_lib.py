@@ -69,6 +69,8 @@ SIGNATURES = {
     "pff_batch_graphflood": (_i32, [_vp, _vp, _vp, _vp, _vp, _f32, _f32, _i32, _i32, _vp, _vp, _vp, _i64, _i32,
                                     _i32, _i32, _vp, _sz, _vp]),
     "pff_conv3x3_fwd": (_i32, [_vp, _i32, _i32, _vp, _vp, _vp, _i32, _i32] + [_i32] * 7 + [_vp]),
+    "pff_receivers_set_path": (_i32, [_i32]),
+    "pff_receivers_div_selfcheck": (_i32, [_f32, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "pff_conv_set_path": (_i32, [_i32]),
     "pff_conv_tc_status": (_i32, [C.POINTER(C.c_int)]),
     "pff_conv3x3_wflip": (_i32, [_vp, _vp, _i32, _i32, _vp]),

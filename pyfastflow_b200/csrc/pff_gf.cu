@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include "pff_internal.h"
+#include "pff_div.cuh"
 
 namespace pff {
 
@@ -32,42 +33,85 @@ __global__ void __launch_bounds__(256) k_fill_round(const float *__restrict__ zh
 // changes (:32 keeps it), so zs[r] is zh[r] there.  Bit 31 of the pointer word marks
 // those cells; a self-pointer made by a receiver cycle (no such bit) reads zh[r].
 constexpr uint32_t FILL_ROOT = 0x80000000u;
+// Rounds from FILL_VOTE0 on record whether any input record was unsettled; a round
+// after one whose input was all settled does nothing (see k_fill_round_packed).
+constexpr int FILL_VOTE0 = 10;
+constexpr int FILL_FLAGS = 64;  // ints after the two record buffers in the workspace
 __global__ void __launch_bounds__(256) k_fill_pack(const float *__restrict__ zh, const int32_t *__restrict__ rcv,
-                                                   uint2 *__restrict__ A, int N)
+                                                   uint2 *__restrict__ A, int N, int *flags)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (flags && blockIdx.x == 0 && threadIdx.x < FILL_FLAGS) flags[threadIdx.x] = 0;
     if (i >= N) return;
     int r = rcv[i];
     if ((unsigned)r >= (unsigned)N) r = i;  // an out-of-range receiver: no read outside the records
     A[i] = make_uint2((uint32_t)r | (r == i ? FILL_ROOT : 0u), __float_as_uint(zh[i]));
 }
 
-__device__ __forceinline__ uint2 fill_step(const float *__restrict__ zh, int i, uint2 me, uint2 at, float inc)
+// One round for cell i: `me` its record, `at` the record at its pointer.  `settled`:
+// the cell is a root, or its pointer reaches a root (rr == r) and it stands above
+// that root's surface, so it keeps its record in this and every later round,
+// whatever the increment.
+__device__ __forceinline__ uint2 fill_step(const float *__restrict__ zh, int i, uint2 me, uint2 at, float inc,
+                                           bool &settled)
 {
     const int r = (int)(me.x & ~FILL_ROOT);
     const int rr = (int)(at.x & ~FILL_ROOT);
     const float zi = __uint_as_float(me.y), zr = __uint_as_float(at.y);
     float zn;
+    settled = true;
     if (i == r) zn = zi;
     else if (rr == r && zi > ((at.x & FILL_ROOT) ? zr : zh[r])) zn = zi;  // :32
-    else zn = fmaxf(zi, __fadd_rn(zr, inc));                              // :36
+    else {
+        zn = fmaxf(zi, __fadd_rn(zr, inc));                               // :36
+        settled = false;
+    }
     return make_uint2((uint32_t)rr | (me.x & FILL_ROOT), __float_as_uint(zn));  // :29
 }
 
-// two cells per thread (i and i + 256 in a block's 512): both gathers in flight at once
+// Two cells per thread (i and i + 256 in a block's 512): both gathers in flight at once.
 __global__ void __launch_bounds__(256) k_fill_round_packed(const float *__restrict__ zh, const uint2 *__restrict__ A,
                                                            uint2 *__restrict__ B, float inc, int N)
 {
     const int i0 = blockIdx.x * 512 + threadIdx.x, i1 = i0 + 256;
+    bool s0, s1;
     if (i1 < N) {
         const uint2 m0 = A[i0], m1 = A[i1];
         const uint2 a0 = A[m0.x & ~FILL_ROOT], a1 = A[m1.x & ~FILL_ROOT];
-        B[i0] = fill_step(zh, i0, m0, a0, inc);
-        B[i1] = fill_step(zh, i1, m1, a1, inc);
+        B[i0] = fill_step(zh, i0, m0, a0, inc, s0);
+        B[i1] = fill_step(zh, i1, m1, a1, inc, s1);
     } else if (i0 < N) {
         const uint2 m0 = A[i0];
-        B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc);
+        B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc, s0);
     }
+}
+
+// The rounds from FILL_VOTE0 on: the same step over a grid-stride loop with a few
+// blocks per SM, each block recording in flags[it] whether any input record it read
+// was unsettled (one atomic per block at most, after a read of the flag).  If the
+// input of round it-1 was all settled, round it-1 copied every record unchanged and
+// so would every later round: round it then returns at once (both record buffers
+// already hold the final records), as do the later rounds, whose flags stay 0.
+__global__ void __launch_bounds__(256) k_fill_round_late(const float *__restrict__ zh, const uint2 *__restrict__ A,
+                                                         uint2 *__restrict__ B, float inc, int N, int *flags, int it)
+{
+    if (it > FILL_VOTE0 && *(volatile const int *)&flags[it - 1] == 0) return;
+    bool uns = false;
+    for (int i0 = blockIdx.x * 512 + threadIdx.x; i0 < N; i0 += gridDim.x * 512) {
+        const int i1 = i0 + 256;
+        bool s0 = true, s1 = true;
+        if (i1 < N) {
+            const uint2 m0 = A[i0], m1 = A[i1];
+            const uint2 a0 = A[m0.x & ~FILL_ROOT], a1 = A[m1.x & ~FILL_ROOT];
+            B[i0] = fill_step(zh, i0, m0, a0, inc, s0);
+            B[i1] = fill_step(zh, i1, m1, a1, inc, s1);
+        } else {
+            const uint2 m0 = A[i0];
+            B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc, s0);
+        }
+        uns |= !(s0 && s1);
+    }
+    if (__syncthreads_or(uns) && threadIdx.x == 0 && *(volatile int *)&flags[it] == 0) atomicOr(&flags[it], 1);
 }
 
 // the packed result to z_ and both receiver buffers (:39-40), then, if h is given,
@@ -197,14 +241,19 @@ __device__ __forceinline__ bool df_inside(const Grid &g, int r, int c)
 }
 __device__ __forceinline__ int df_wrap(int v, int n) { return (v >= 0 && v < n) ? v : ((v % n) + n) % n; }
 
-__device__ __forceinline__ float df_add(float acc, unsigned char f, float w, float q)
+
+// The weight stored for a link whose source is not a source cell (a boundary cell,
+// one outside the domain, or one with sums == 0): real weights are >= 0 or NaN.
+constexpr float DF_SKIP = -1.0f;
+__device__ __forceinline__ float df_add(float acc, float w, float q)
 {
-    return (f & 2) ? __fadd_rn(acc, __fmul_rn(w, q)) : acc;
+    const float t = __fadd_rn(acc, __fmul_rn(w, q));
+    return w != DF_SKIP ? t : acc;
 }
 
 template <int MODE, int H>
 __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__ zh, const float *__restrict__ Qin,
-                                                       float *__restrict__ out, Grid g, float dx, float prec_dx2)
+                                                       float *__restrict__ out, Grid g, DivC dc, float prec_dx2)
 {
     constexpr int RX = DF_TX + 2 * H, RY = DF_TY + 2 * H, ZX = RX + 2, ZY = RY + 2, P = RX * RY;
     extern __shared__ __align__(16) float df_sm[];
@@ -213,23 +262,35 @@ __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__
     float *qa = w3 + P, *qb = qa + P;
     unsigned char *fl = reinterpret_cast<unsigned char *>(qb + P);
     const int x0 = blockIdx.x * DF_TX - H, y0 = blockIdx.y * DF_TY - H;  // region origin (unwrapped)
-    for (int t = threadIdx.x; t < ZX * ZY; t += blockDim.x) {
-        const int r = y0 - 1 + t / ZX, c = x0 - 1 + t % ZX;
-        zs[t] = df_inside<MODE>(g, r, c) ? zh[df_wrap(r, g.ny) * g.nx + df_wrap(c, g.nx)] : 0.f;
+    const int nx = g.nx, ny = g.ny;
+    // the region and its ring strictly inside the grid: every region cell is an interior
+    // cell (all four neighbours, none on the edge), no wrapping, no domain checks
+    const bool inner = x0 >= 1 && y0 >= 1 && x0 + RX < nx && y0 + RY < ny;
+    if (inner) {
+        for (int t = threadIdx.x; t < ZX * ZY; t += blockDim.x)
+            zs[t] = zh[(size_t)(y0 - 1 + t / ZX) * nx + x0 - 1 + t % ZX];
+    } else {
+        for (int t = threadIdx.x; t < ZX * ZY; t += blockDim.x) {
+            const int r = y0 - 1 + t / ZX, c = x0 - 1 + t % ZX;
+            zs[t] = df_inside<MODE>(g, r, c) ? zh[df_wrap(r, ny) * nx + df_wrap(c, nx)] : 0.f;
+        }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < P; t += blockDim.x) {
         const int ry = t / RX, rx = t % RX, r = y0 + ry, c = x0 + rx;
         unsigned char f = 0;
-        float q = 0.f, wk[4] = {0.f, 0.f, 0.f, 0.f};
-        if (df_inside<MODE>(g, r, c)) {
-            const int row = df_wrap(r, g.ny), col = df_wrap(c, g.nx);
-            q = Qin[row * g.nx + col];
+        float q = 0.f, wk[4] = {DF_SKIP, DF_SKIP, DF_SKIP, DF_SKIP};
+        if (inner || df_inside<MODE>(g, r, c)) {
+            const int row = inner ? r : df_wrap(r, ny), col = inner ? c : df_wrap(c, nx);
+            q = Qin[row * nx + col];
             f = 1;
-            const bool redge = row == 0 || row == g.ny - 1, cedge = col == 0 || col == g.nx - 1;
-            if (MODE == 1 && cedge) f |= 1 << 2;
-            if (MODE == 2 && redge) f |= (row == 0 ? 2 : 3) << 2;
-            const bool leave = MODE == 0 ? (redge || cedge) : (MODE == 1 ? redge : cedge);
+            bool leave = false;
+            if (!inner) {
+                const bool redge = row == 0 || row == ny - 1, cedge = col == 0 || col == nx - 1;
+                if (MODE == 1 && cedge) f |= 1 << 2;
+                if (MODE == 2 && redge) f |= (row == 0 ? 2 : 3) << 2;
+                leave = MODE == 0 ? (redge || cedge) : (MODE == 1 ? redge : cedge);
+            }
             if (!leave) {  // all four neighbours exist
                 const int z = (ry + 1) * ZX + rx + 1;
                 const float zi = zs[z];
@@ -240,11 +301,10 @@ __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__
                 // only the descending links divide
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    sk[k] = zi > zn[k] ? fmaxf(0.f, __fdiv_rn(__fsub_rn(zi, zn[k]), dx)) : 0.f;
+                    sk[k] = zi > zn[k] ? fmaxf(0.f, div_dx(__fsub_rn(zi, zn[k]), dc)) : 0.f;
                     sums = __fadd_rn(sums, sk[k]);
                 }
                 if (sums != 0.f) {
-                    f |= 2;
 #pragma unroll
                     for (int k = 0; k < 4; ++k) wk[k] = sk[k] != 0.f ? __fdiv_rn(sk[k], sums) : 0.f;
                 }
@@ -267,33 +327,34 @@ __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__
             const unsigned char f = fl[i];
             if (!(f & 1)) continue;
             // the source above reaches i through its bottom link (w3), the left one
-            // through its right link (w2), the right one its left (w1), below its top (w0)
+            // through its right link (w2), the right one its left (w1), below its top (w0);
+            // a neighbour that is not a source has the weight DF_SKIP on every link
             const int u = i - RX, l = i - 1, rt = i + 1, d = i + RX;
             float acc = prec_dx2;
             switch (f >> 2) {
             case 0:
-                acc = df_add(acc, fl[u], w3[u], qc[u]);
-                acc = df_add(acc, fl[l], w2[l], qc[l]);
-                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
-                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                acc = df_add(acc, w3[u], qc[u]);
+                acc = df_add(acc, w2[l], qc[l]);
+                acc = df_add(acc, w1[rt], qc[rt]);
+                acc = df_add(acc, w0[d], qc[d]);
                 break;
             case 1:
-                acc = df_add(acc, fl[u], w3[u], qc[u]);
-                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
-                acc = df_add(acc, fl[l], w2[l], qc[l]);
-                acc = df_add(acc, fl[d], w0[d], qc[d]);
+                acc = df_add(acc, w3[u], qc[u]);
+                acc = df_add(acc, w1[rt], qc[rt]);
+                acc = df_add(acc, w2[l], qc[l]);
+                acc = df_add(acc, w0[d], qc[d]);
                 break;
             case 2:
-                acc = df_add(acc, fl[l], w2[l], qc[l]);
-                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
-                acc = df_add(acc, fl[d], w0[d], qc[d]);
-                acc = df_add(acc, fl[u], w3[u], qc[u]);
+                acc = df_add(acc, w2[l], qc[l]);
+                acc = df_add(acc, w1[rt], qc[rt]);
+                acc = df_add(acc, w0[d], qc[d]);
+                acc = df_add(acc, w3[u], qc[u]);
                 break;
             default:
-                acc = df_add(acc, fl[d], w0[d], qc[d]);
-                acc = df_add(acc, fl[u], w3[u], qc[u]);
-                acc = df_add(acc, fl[l], w2[l], qc[l]);
-                acc = df_add(acc, fl[rt], w1[rt], qc[rt]);
+                acc = df_add(acc, w0[d], qc[d]);
+                acc = df_add(acc, w3[u], qc[u]);
+                acc = df_add(acc, w2[l], qc[l]);
+                acc = df_add(acc, w1[rt], qc[rt]);
                 break;
             }
             qn[i] = acc;
@@ -306,7 +367,7 @@ __global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__
     for (int t = threadIdx.x; t < DF_TX * DF_TY; t += blockDim.x) {
         const int ly = t / DF_TX, lx = t % DF_TX;
         const int row = y0 + H + ly, col = x0 + H + lx;
-        if (row < g.ny && col < g.nx) out[row * g.nx + col] = qc[(H + ly) * RX + H + lx];
+        if (row < ny && col < nx) out[row * nx + col] = qc[(H + ly) * RX + H + lx];
     }
 }
 
@@ -318,7 +379,7 @@ static int l_diffuse_fused_h(const float *zh, float *Q, float *temp, const Grid 
                                   (int)df_smem(H)));
     dim3 gr(div_up(g.nx, DF_TX), div_up(g.ny, DF_TY));
     PFF_PROBED("k_diffuse_fused", st,
-               k_diffuse_fused<MODE, H><<<gr, 256, df_smem(H), st>>>(zh, Q, temp, g, dx, prec_dx2));
+               k_diffuse_fused<MODE, H><<<gr, 256, df_smem(H), st>>>(zh, Q, temp, g, make_divc(dx), prec_dx2));
     count_launch();
     return PFF_OK;
 }
@@ -480,7 +541,7 @@ static bool g_diffuse_unfused = getenv("PFF_DIFFUSE_UNFUSED") != nullptr;  // di
 extern "C" size_t pff_fill_workspace_bytes(int N)
 {
     if (N < 1) return 256;
-    return 2 * Carver::round(sizeof(uint2) * (size_t)N) + 256;
+    return 2 * Carver::round(sizeof(uint2) * (size_t)N) + Carver::round(sizeof(int) * FILL_FLAGS);
 }
 
 // ceil(log2 N) rounds (:121) of the packed fill; `inc(it)` is round it's increment.
@@ -491,11 +552,24 @@ static uint2 *fill_rounds(const float *zh, const int32_t *receivers, void *works
 {
     Carver cv(workspace, workspace_bytes);
     uint2 *a = cv.take<uint2>(N), *b = cv.take<uint2>(N);
-    { k_fill_pack<<<div_up(N, 256), 256, 0, st>>>(zh, receivers, a, N); count_launch(); }  // :116-117
+    int *flags = cv.take<int>(FILL_FLAGS);
+    { k_fill_pack<<<div_up(N, 256), 256, 0, st>>>(zh, receivers, a, N, flags); count_launch(); }  // :116-117
     int nr = 0;
     for (long long p = 1; p < N; p <<= 1) ++nr;
+    int late_blocks = 0;
+    if (nr > FILL_VOTE0) {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        late_blocks = std::min(div_up(N, 512), 8 * sms);
+    }
     for (int it = 0; it < nr; ++it) {
-        PFF_PROBED("k_fill_round_packed", st, k_fill_round_packed<<<div_up(N, 512), 256, 0, st>>>(zh, a, b, inc(it), N));
+        if (it < FILL_VOTE0) {
+            PFF_PROBED("k_fill_round_packed", st,
+                       k_fill_round_packed<<<div_up(N, 512), 256, 0, st>>>(zh, a, b, inc(it), N));
+        } else {
+            PFF_PROBED("k_fill_round_late", st,
+                       k_fill_round_late<<<late_blocks, 256, 0, st>>>(zh, a, b, inc(it), N, flags, it));
+        }
         count_launch();
         std::swap(a, b);
     }

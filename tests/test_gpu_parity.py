@@ -100,6 +100,56 @@ def test_receivers(orc, cuda, mode, kind):
         assert np.array_equal(fbits(host(gr)), fbits(go))
 
 
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_receivers_lean_kernel_variants(orc, cuda, mode):
+    """Both variants of the lean receivers kernel (7 and 8 CTAs per SM) and the
+    earlier 4-column walk against the oracle: single- and
+    partial-strip widths, one- and many-band heights, 2-row grids, integer ties,
+    near ties (drops a few ulps apart), tiny and huge cell sizes."""
+    torch = cuda
+    from pyfastflow_b200 import _lib, flow
+
+    lib = _lib.load()
+    cases = [(4, 2, "int", 30.0), (8, 3, "uniform", 3.0), (516, 77, "int", 30.0), (1024, 130, "spectral", 3.0),
+             (2048, 70, "uniform", 1e-30), (1536, 9, "int", 1e30), (256, 40, "near", 10.0), (132, 33, "near", 0.3)]
+    try:
+        for (nx, ny, kind, dx) in cases:
+            g = Grid(orc, torch, nx, ny, mode, seed=nx)
+            if kind == "near":  # neighbours within a few ulps of each other: ties after rounding
+                rng = np.random.default_rng(nx)
+                base = np.float32(1000.0) + (rng.integers(0, 3, (ny, nx)) * np.float32(0.5)).astype(np.float32)
+                z = (base.view(np.uint32) + rng.integers(-6, 7, (ny, nx)).astype(np.uint32)).view(np.float32)
+            else:
+                z = make_case(kind, nx, ny, seed=ny + mode)
+            set_constants(g, dx)
+            zd = dev(torch, z.ravel())
+            ro, go = orc.compute_receivers(z, g.og, dx)
+            for path in (1, 2, 0):
+                lib.pff_receivers_set_path(path)
+                r = torch.full((g.N,), -7, dtype=torch.int32, device="cuda")
+                gr = torch.full((g.N,), -7.0, dtype=torch.float32, device="cuda")
+                flow.compute_receivers(zd, r, gr)
+                assert np.array_equal(host(r), ro), (nx, ny, kind, path)
+                assert np.array_equal(fbits(host(gr)), fbits(go)), (nx, ny, kind, path)
+    finally:
+        lib.pff_receivers_set_path(1)
+
+
+@pytest.mark.parametrize("dx", [30.0, 10.0, 3.0, 1.0, 0.3, 7.77, 123.456, 1e-3, 3e-20, 1e4, 0.1, 2.0 ** -20])
+def test_receivers_division_exhaustive(cuda, dx):
+    """The lean kernel's Markstein-corrected quotient equals the IEEE division for
+    every float in the range of drops it is used for."""
+    import ctypes as C
+
+    from pyfastflow_b200 import _lib
+
+    lib = _lib.load()
+    bad, n = C.c_longlong(-1), C.c_longlong(0)
+    assert lib.pff_receivers_div_selfcheck(np.float32(dx), C.byref(bad), C.byref(n)) == 0
+    assert n.value > (100 << 23), n.value  # 135-200 binades of drops, by dx
+    assert bad.value == 0
+
+
 @pytest.mark.parametrize("mode", MODES)
 def test_basin_labels(orc, cuda, mode):
     torch = cuda

@@ -400,18 +400,19 @@ __device__ __noinline__ int2 rcv_scan_dir(float d0, float d1, float d2, float d3
 // Fast choice from the four drops (-inf for an invalid link): the direction (-1: the
 // cell is its own receiver) and the gradient; `ok` false when the ordered scan must
 // decide instead.
-__device__ __forceinline__ int rcv_dir_fast(float d0, float d1, float d2, float d3, const DivC &c, float &s, bool &ok)
+__device__ __forceinline__ int rcv_off_fast(float d0, float d1, float d2, float d3, int ot, int ow, int oe, int ob,
+                                            const DivC &c, float &s, bool &ok)
 {
     const float m = fmaxf(fmaxf(d0, d1), fmaxf(d2, d3));  // NaN drops are ignored, as by '>'
     const float near = __fmul_rn(m, 1.0f - 0x1p-21f);
     const bool p0 = d0 >= near, p1 = d1 >= near, p2 = d2 >= near;
     const float dsel = p0 ? d0 : (p1 ? d1 : (p2 ? d2 : d3));
-    const int k = p0 ? 0 : (p1 ? 1 : (p2 ? 2 : 3));
+    const int off = p0 ? ot : (p1 ? ow : (p2 ? oe : ob));
     const float q = div_markstein(m, c);
     const bool pit = !(m > 0.f);  // pit or flat (or all drops NaN / invalid)
     ok = pit || (dsel == m && m >= c.mlo && m <= c.mhi);
     s = pit ? 0.f : q;
-    return pit ? -1 : k;
+    return pit ? 0 : off;
 }
 
 template <int MODE, int RL_P, int MINB>
@@ -486,10 +487,11 @@ __global__ void __launch_bounds__(128, MINB) k_receivers_lean(const float *__res
             float zr = __shfl_down_sync(0xffffffffu, zc.x, 1);
             if (lhalo) zl = hl;
             if (rhalo) zr = hr;
-            const bool tvalid = r > 0 || MODE == 2, bvalid = r < ny - 1 || MODE == 2;
             const float n0 = __fsub_rn(zc.x, zb.x), n1 = __fsub_rn(zc.y, zb.y), n2 = __fsub_rn(zc.z, zb.z),
                         n3 = __fsub_rn(zc.w, zb.w);  // bottom drops
-            if (incol) {
+            // the four cells of this row; tvalid / bvalid: the row has a north / south
+            // neighbour row; offt / offb: the receiver offsets of those links
+            auto cells = [&](bool tvalid, bool bvalid, int offt, int offb) {
                 const float t0 = tvalid ? -db0 : NEG, t1 = tvalid ? -db1 : NEG, t2 = tvalid ? -db2 : NEG,
                             t3 = tvalid ? -db3 : NEG;
                 const float b0 = bvalid ? n0 : NEG, b1 = bvalid ? n1 : NEG, b2 = bvalid ? n2 : NEG,
@@ -499,28 +501,30 @@ __global__ void __launch_bounds__(128, MINB) k_receivers_lean(const float *__res
                 const float l0 = lvalid ? __fsub_rn(zc.x, zl) : NEG;  // west drop of the first cell
                 float s0, s1, s2, s3;
                 bool ok0, ok1, ok2, ok3;
-                int k0 = rcv_dir_fast(t0, l0, e0, b0, c, s0, ok0);
-                int k1 = rcv_dir_fast(t1, -e0, e1, b1, c, s1, ok1);
-                int k2 = rcv_dir_fast(t2, -e1, e2, b2, c, s2, ok2);
-                int k3 = rcv_dir_fast(t3, -e2, e3, b3, c, s3, ok3);
+                int o0 = rcv_off_fast(t0, l0, e0, b0, offt, offl, 1, offb, c, s0, ok0);
+                int o1 = rcv_off_fast(t1, -e0, e1, b1, offt, -1, 1, offb, c, s1, ok1);
+                int o2 = rcv_off_fast(t2, -e1, e2, b2, offt, -1, 1, offb, c, s2, ok2);
+                int o3 = rcv_off_fast(t3, -e2, e3, b3, offt, -1, offr, offb, c, s3, ok3);
                 if (!(ok0 && ok1 && ok2 && ok3)) {  // rare: near ties or drops outside the exact-division range
+                    auto off = [&](int k, int ow, int oe) {
+                        return k < 0 ? 0 : (k == 0 ? offt : (k == 1 ? ow : (k == 2 ? oe : offb)));
+                    };
                     int2 v;
-                    if (!ok0) { v = rcv_scan_dir(t0, l0, e0, b0, c.dx); k0 = v.x; s0 = __int_as_float(v.y); }
-                    if (!ok1) { v = rcv_scan_dir(t1, -e0, e1, b1, c.dx); k1 = v.x; s1 = __int_as_float(v.y); }
-                    if (!ok2) { v = rcv_scan_dir(t2, -e1, e2, b2, c.dx); k2 = v.x; s2 = __int_as_float(v.y); }
-                    if (!ok3) { v = rcv_scan_dir(t3, -e2, e3, b3, c.dx); k3 = v.x; s3 = __int_as_float(v.y); }
+                    if (!ok0) { v = rcv_scan_dir(t0, l0, e0, b0, c.dx); o0 = off(v.x, offl, 1); s0 = __int_as_float(v.y); }
+                    if (!ok1) { v = rcv_scan_dir(t1, -e0, e1, b1, c.dx); o1 = off(v.x, -1, 1); s1 = __int_as_float(v.y); }
+                    if (!ok2) { v = rcv_scan_dir(t2, -e1, e2, b2, c.dx); o2 = off(v.x, -1, 1); s2 = __int_as_float(v.y); }
+                    if (!ok3) { v = rcv_scan_dir(t3, -e2, e3, b3, c.dx); o3 = off(v.x, -1, offr); s3 = __int_as_float(v.y); }
                 }
-                // receiver offsets by direction (top / bottom wrap in periodic north-south)
-                const int offt = (MODE == 2 && r == 0) ? (ny - 1) * nx : -nx;
-                const int offb = (MODE == 2 && r == ny - 1) ? -(ny - 1) * nx : nx;
                 const int i0 = r * nx + c0;
-                auto recv = [&](int k, int i, int ow, int oe) -> int {
-                    return k < 0 ? i : i + (k == 0 ? offt : (k == 1 ? ow : (k == 2 ? oe : offb)));
-                };
                 const size_t o = (size_t)r * nx4 + q0;
-                reinterpret_cast<int4 *>(rcv)[o] = make_int4(recv(k0, i0, offl, 1), recv(k1, i0 + 1, -1, 1),
-                                                             recv(k2, i0 + 2, -1, 1), recv(k3, i0 + 3, -1, offr));
+                reinterpret_cast<int4 *>(rcv)[o] = make_int4(i0 + o0, i0 + 1 + o1, i0 + 2 + o2, i0 + 3 + o3);
                 reinterpret_cast<float4 *>(grad)[o] = make_float4(s0, s1, s2, s3);
+            };
+            if (incol) {
+                if (r > 0 && r < ny - 1) cells(true, true, -nx, nx);  // an interior row
+                else  // the first or last row (wrapped links in periodic north-south)
+                    cells(r > 0 || MODE == 2, r < ny - 1 || MODE == 2, (MODE == 2 && r == 0) ? (ny - 1) * nx : -nx,
+                          (MODE == 2 && r == ny - 1) ? -(ny - 1) * nx : nx);
             }
             db0 = n0;
             db1 = n1;

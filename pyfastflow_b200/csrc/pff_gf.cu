@@ -69,21 +69,42 @@ __device__ __forceinline__ uint2 fill_step(const float *__restrict__ zh, int i, 
     return make_uint2((uint32_t)rr | (me.x & FILL_ROOT), __float_as_uint(zn));  // :29
 }
 
-// Two cells per thread (i and i + 256 in a block's 512): both gathers in flight at once.
+// FILL_CPT cells per thread (i, i + 256, ... in a block's 256 * FILL_CPT): all their
+// records are read, then all the gathers at their pointers are in flight at once (the
+// rounds are bound by the latency of that dependent gather).  Returns whether any
+// input record was unsettled.
+constexpr int FILL_CPT = 4;
+__device__ __forceinline__ bool fill_cells(const float *__restrict__ zh, const uint2 *__restrict__ A,
+                                           uint2 *__restrict__ B, float inc, int N, int base)
+{
+    uint2 m[FILL_CPT], at[FILL_CPT];
+#pragma unroll
+    for (int k = 0; k < FILL_CPT; ++k) {
+        const int i = base + threadIdx.x + 256 * k;
+        m[k] = i < N ? A[i] : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < FILL_CPT; ++k) {
+        const int i = base + threadIdx.x + 256 * k;
+        at[k] = i < N ? A[m[k].x & ~FILL_ROOT] : make_uint2(0u, 0u);
+    }
+    bool uns = false;
+#pragma unroll
+    for (int k = 0; k < FILL_CPT; ++k) {
+        const int i = base + threadIdx.x + 256 * k;
+        if (i < N) {
+            bool st;
+            B[i] = fill_step(zh, i, m[k], at[k], inc, st);
+            uns |= !st;
+        }
+    }
+    return uns;
+}
+
 __global__ void __launch_bounds__(256) k_fill_round_packed(const float *__restrict__ zh, const uint2 *__restrict__ A,
                                                            uint2 *__restrict__ B, float inc, int N)
 {
-    const int i0 = blockIdx.x * 512 + threadIdx.x, i1 = i0 + 256;
-    bool s0, s1;
-    if (i1 < N) {
-        const uint2 m0 = A[i0], m1 = A[i1];
-        const uint2 a0 = A[m0.x & ~FILL_ROOT], a1 = A[m1.x & ~FILL_ROOT];
-        B[i0] = fill_step(zh, i0, m0, a0, inc, s0);
-        B[i1] = fill_step(zh, i1, m1, a1, inc, s1);
-    } else if (i0 < N) {
-        const uint2 m0 = A[i0];
-        B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc, s0);
-    }
+    fill_cells(zh, A, B, inc, N, blockIdx.x * (256 * FILL_CPT));
 }
 
 // The rounds from FILL_VOTE0 on: the same step over a grid-stride loop with a few
@@ -97,20 +118,8 @@ __global__ void __launch_bounds__(256) k_fill_round_late(const float *__restrict
 {
     if (it > FILL_VOTE0 && *(volatile const int *)&flags[it - 1] == 0) return;
     bool uns = false;
-    for (int i0 = blockIdx.x * 512 + threadIdx.x; i0 < N; i0 += gridDim.x * 512) {
-        const int i1 = i0 + 256;
-        bool s0 = true, s1 = true;
-        if (i1 < N) {
-            const uint2 m0 = A[i0], m1 = A[i1];
-            const uint2 a0 = A[m0.x & ~FILL_ROOT], a1 = A[m1.x & ~FILL_ROOT];
-            B[i0] = fill_step(zh, i0, m0, a0, inc, s0);
-            B[i1] = fill_step(zh, i1, m1, a1, inc, s1);
-        } else {
-            const uint2 m0 = A[i0];
-            B[i0] = fill_step(zh, i0, m0, A[m0.x & ~FILL_ROOT], inc, s0);
-        }
-        uns |= !(s0 && s1);
-    }
+    for (int base = blockIdx.x * (256 * FILL_CPT); base < N; base += gridDim.x * (256 * FILL_CPT))
+        uns |= fill_cells(zh, A, B, inc, N, base);
     if (__syncthreads_or(uns) && threadIdx.x == 0 && *(volatile int *)&flags[it] == 0) atomicOr(&flags[it], 1);
 }
 
@@ -211,7 +220,7 @@ __global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__
 }
 
 // ---- diffusion, all sweeps in one pass (boundary modes 0-2) -----------------------
-// A 64 x 16 tile with a halo of H = nsweeps cells: sweep s is valid on the region
+// A 64 x 32 tile (512 threads) with a halo of H = nsweeps cells: sweep s is valid on the region
 // shrunk by s, so after H sweeps the tile itself is exact.  Per block: zh over the
 // region and one more ring (the weights of the region's cells need their
 // neighbours), then each region cell's four outgoing weights and source flag
@@ -228,7 +237,7 @@ __global__ void __launch_bounds__(256) k_diffuse_sweep(const float *__restrict__
 // nx-1: top, right, left, bottom; periodic NS row 0: left, right, bottom, top; row
 // ny-1: bottom, top, left, right.  Flag byte per region cell: bit 0 in the grid,
 // bit 1 a source, bits 2-3 that order.
-constexpr int DF_TX = 64, DF_TY = 16, DF_HMAX = 8;
+constexpr int DF_TX = 64, DF_TY = 32, DF_HMAX = 8, DF_THREADS = 512;
 __host__ __device__ constexpr int df_region(int H) { return (DF_TX + 2 * H) * (DF_TY + 2 * H); }
 __host__ __device__ constexpr int df_ring(int H) { return (DF_TX + 2 * H + 2) * (DF_TY + 2 * H + 2); }
 // zh over the region and its ring, four weight planes, two Q buffers, the flags
@@ -252,7 +261,7 @@ __device__ __forceinline__ float df_add(float acc, float w, float q)
 }
 
 template <int MODE, int H>
-__global__ void __launch_bounds__(256) k_diffuse_fused(const float *__restrict__ zh, const float *__restrict__ Qin,
+__global__ void __launch_bounds__(DF_THREADS) k_diffuse_fused(const float *__restrict__ zh, const float *__restrict__ Qin,
                                                        float *__restrict__ out, Grid g, DivC dc, float prec_dx2)
 {
     constexpr int RX = DF_TX + 2 * H, RY = DF_TY + 2 * H, ZX = RX + 2, ZY = RY + 2, P = RX * RY;
@@ -379,7 +388,7 @@ static int l_diffuse_fused_h(const float *zh, float *Q, float *temp, const Grid 
                                   (int)df_smem(H)));
     dim3 gr(div_up(g.nx, DF_TX), div_up(g.ny, DF_TY));
     PFF_PROBED("k_diffuse_fused", st,
-               k_diffuse_fused<MODE, H><<<gr, 256, df_smem(H), st>>>(zh, Q, temp, g, make_divc(dx), prec_dx2));
+               k_diffuse_fused<MODE, H><<<gr, DF_THREADS, df_smem(H), st>>>(zh, Q, temp, g, make_divc(dx), prec_dx2));
     count_launch();
     return PFF_OK;
 }
@@ -560,12 +569,12 @@ static uint2 *fill_rounds(const float *zh, const int32_t *receivers, void *works
     if (nr > FILL_VOTE0) {
         int dev = 0, sms = 148;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        late_blocks = std::min(div_up(N, 512), 8 * sms);
+        late_blocks = std::min(div_up(N, 256 * FILL_CPT), 8 * sms);
     }
     for (int it = 0; it < nr; ++it) {
         if (it < FILL_VOTE0) {
             PFF_PROBED("k_fill_round_packed", st,
-                       k_fill_round_packed<<<div_up(N, 512), 256, 0, st>>>(zh, a, b, inc(it), N));
+                       k_fill_round_packed<<<div_up(N, 256 * FILL_CPT), 256, 0, st>>>(zh, a, b, inc(it), N));
         } else {
             PFF_PROBED("k_fill_round_late", st,
                        k_fill_round_late<<<late_blocks, 256, 0, st>>>(zh, a, b, inc(it), N, flags, it));

@@ -47,6 +47,7 @@ KERNELS = {
     "k_receivers": (12, 152.3e6),           # z in; receivers + gradient out
     "k_tile_terminal<grid>": (8, None),     # receivers in; tile terminals out
     "k_tile_terminal<list>": (None, None),  # the tiles a carve changed
+    "k_saddle_p12_strip": (13, None),       # labels + z in; is_border + z' out (the border lists are extra)
     "k_tree_tile<up>": (8, 251.0e6),        # receivers + seeds in
     "k_tree_tile<down>": (16, 323.0e6),     # receivers + seeds in; Q + counts out
 }
@@ -871,6 +872,7 @@ GF_KERNELS = {
     "k_receivers": 12,            # zh in; receivers + gradient out
     "k_tile_terminal<grid>": 8,   # receivers in; tile terminals out
     "k_tile_terminal<list>": None,
+    "k_relabel_jump_block": None,  # one CTA: the basin chains of a short pit list
     "k_fill_round_packed": 16,    # one 8-byte {pointer, z} record in and out per round (the gather at the pointer is extra)
     "k_fill_round_late": 16,      # the same rounds from the tenth on (a round after a settled one returns at once)
     "k_diffuse_fused": 12,        # zh + Q in; Q after all sweeps out

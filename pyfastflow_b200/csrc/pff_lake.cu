@@ -549,7 +549,12 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
         zc = z[row0 * nx + col];
         if (row0 > 0) { ba = bid[(row0 - 1) * nx + col]; za = z[(row0 - 1) * nx + col]; }
     }
-    const bool hl = lane == 0 && col > 0 && incol, hr = lane == 31 && col + 1 < nx && incol;
+    // strip-edge halo columns; in periodic east-west the grid's first and last columns
+    // take the wrapped column, so that they run the interior path too (no warp of the
+    // edge strips waits on per-row neighbour loads)
+    const bool hl = lane == 0 && incol && (col > 0 || MODE == 1);
+    const bool hr = (lane == 31 || col == nx - 1) && incol && (col + 1 < nx || MODE == 1);
+    const int lcol = col > 0 ? col - 1 : nx - 1, rcol = col + 1 < nx ? col + 1 : 0;
     for (int row = row0; row < row1; row += SAD_AHEAD) {
         // the rows below (and the strip-edge halo) of SAD_AHEAD rows, loaded together
         int bq[SAD_AHEAD], lq[SAD_AHEAD], rq[SAD_AHEAD];
@@ -561,10 +566,10 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
             bq[q] = vb ? bid[rb * nx + col] : 0;
             zq[q] = vb ? z[rb * nx + col] : 0.f;
             const bool vl = hl && rc < row1, vr = hr && rc < row1;
-            lq[q] = vl ? bid[rc * nx + col - 1] : 0;
-            zlq[q] = vl ? z[rc * nx + col - 1] : 0.f;
-            rq[q] = vr ? bid[rc * nx + col + 1] : 0;
-            zrq[q] = vr ? z[rc * nx + col + 1] : 0.f;
+            lq[q] = vl ? bid[rc * nx + lcol] : 0;
+            zlq[q] = vl ? z[rc * nx + lcol] : 0.f;
+            rq[q] = vr ? bid[rc * nx + rcol] : 0;
+            zrq[q] = vr ? z[rc * nx + rcol] : 0.f;
         }
 #pragma unroll
         for (int q = 0; q < SAD_AHEAD; ++q) {
@@ -579,12 +584,14 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
             long long key = 0;
             bool has = false;
             if (incol) {
-                const bool interior = MODE != 3 && rw > 0 && rw < ny - 1 && col > 0 && col < nx - 1;
+                const bool interior =
+                    MODE != 3 && rw > 0 && rw < ny - 1 && (MODE == 1 || (col > 0 && col < nx - 1));
                 if (interior) {
-                    if (lane == 0) { bl = lq[q]; zl = zlq[q]; }
-                    if (lane == 31) { br = rq[q]; zr = zrq[q]; }
-                    // interior cells of modes 0-2 never leave the domain
-                    const int jn[4] = {i - nx, i - 1, i + 1, i + nx};
+                    if (hl) { bl = lq[q]; zl = zlq[q]; }
+                    if (hr) { br = rq[q]; zr = zrq[q]; }
+                    // interior cells of modes 0-2 never leave the domain (east-west links wrap in mode 1)
+                    const int jn[4] = {i - nx, col > 0 ? i - 1 : i + nx - 1, col < nx - 1 ? i + 1 : i - nx + 1,
+                                       i + nx};
                     const int bn[4] = {ba, bl, br, bb};
                     const float zn[4] = {za, zl, zr, zb};
                     listed = saddle_cell<MODE>(i, rw, col, g, bc, zc, jn, bn, zn, is_border, zp, key, has);
@@ -982,8 +989,9 @@ __global__ void k_relabel_init(int32_t *fin, const int32_t *__restrict__ bid, co
 // Inside the reroute graph the block kernel also sets a conditional handle, so the
 // cooperative launch (whose launch alone costs about 10 us) runs only for long lists.
 constexpr int RJ_BLOCK = 16384;
-__global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const int *__restrict__ pits, const int *np,
-                                                            cudaGraphConditionalHandle hj, int set)
+// The one-CTA jump in global memory: the fallback of the shared-memory version below.
+__global__ void __launch_bounds__(1024) k_relabel_jump_global(int32_t *fin, const int *__restrict__ pits,
+                                                              const int *np, cudaGraphConditionalHandle hj, int set)
 {
     const int n = *np;
     if (set && threadIdx.x == 0) cudaGraphSetConditional(hj, n > RJ_BLOCK ? 1u : 0u);
@@ -998,6 +1006,99 @@ __global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const
         }
         if (!__syncthreads_or(ch)) break;
     }
+}
+
+// The same jump with the chains in shared memory.  A target basin is 0 (the outlet
+// basin) or, when the labels are current, a basin of the pit list itself; so the
+// chain is followed over list slots: fin[b] briefly holds b's slot, each pit's target
+// slot is looked up there, and the jumping runs on slots in shared memory (a round
+// costs shared-memory latency instead of two dependent global loads).  A target that
+// is not in the list (labels not current, as after a receiver cycle) restores fin and
+// runs the global-memory rounds instead, so the result is the same in every case.
+constexpr size_t RJ_SMEM = 2 * RJ_BLOCK * sizeof(int);
+__global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const int *__restrict__ pits,
+                                                             const int *np, cudaGraphConditionalHandle hj, int set)
+{
+    extern __shared__ int rj_sm[];
+    int *tgt = rj_sm, *t = rj_sm + RJ_BLOCK;
+    __shared__ int bad;
+    const int n = *np;
+    if (set && threadIdx.x == 0) cudaGraphSetConditional(hj, n > RJ_BLOCK ? 1u : 0u);
+    if (n > RJ_BLOCK) return;
+    if (threadIdx.x == 0) bad = 0;
+    for (int k = threadIdx.x; k < n; k += 1024) tgt[k] = fin[pits[k] + 1];
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += 1024) fin[pits[k] + 1] = k;
+    __syncthreads();  // the block's own global writes are visible to it after the barrier
+    for (int k = threadIdx.x; k < n; k += 1024) {
+        const int x = tgt[k];
+        int sl = -1;
+        if (x != 0) {
+            sl = x > 0 ? fin[x] : -1;
+            if ((unsigned)sl >= (unsigned)n || pits[sl] + 1 != x) {
+                sl = k;
+                bad = 1;
+            }
+        }
+        t[k] = sl;
+    }
+    __syncthreads();
+    if (bad) {  // restore the targets and take the global-memory rounds
+        for (int k = threadIdx.x; k < n; k += 1024) fin[pits[k] + 1] = tgt[k];
+        __syncthreads();
+        for (int r = 0; r < 32; ++r) {
+            bool ch = false;
+            for (int k = threadIdx.x; k < n; k += 1024) {
+                const int b = pits[k] + 1;
+                const int x = fin[b];
+                const int y = fin[x];
+                if (y != x) { fin[b] = y; ch = true; }
+            }
+            if (!__syncthreads_or(ch)) break;
+        }
+        return;
+    }
+    for (int r = 0; r < 32; ++r) {
+        bool ch = false;
+        for (int k = threadIdx.x; k < n; k += 1024) {
+            const int x = t[k];
+            if (x >= 0) {
+                const int y = t[x];
+                if (y != x) { t[k] = y; ch = true; }
+            }
+        }
+        if (!__syncthreads_or(ch)) break;
+    }
+    for (int k = threadIdx.x; k < n; k += 1024) {
+        const int x = t[k];
+        fin[pits[k] + 1] = x < 0 ? 0 : pits[x] + 1;
+    }
+}
+
+// The shared-memory jump needs more than the default 48 KB of dynamic shared memory;
+// the attribute (not a stream operation) is set once per device by the reroute's entry
+// points before they launch anything.  Without it the global-memory kernel runs.
+static bool g_rj_smem[64];
+static void rj_prepare()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || g_rj_smem[dev]) return;
+    if (cudaFuncSetAttribute(k_relabel_jump_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RJ_SMEM) ==
+        cudaSuccess)
+        g_rj_smem[dev] = true;
+    else
+        cudaGetLastError();
+}
+static void launch_relabel_jump_block(int32_t *fin, const int *pits, const int *np, cudaGraphConditionalHandle hj,
+                                      int set, cudaStream_t st)
+{
+    int dev = 0;
+    const bool sm = cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && g_rj_smem[dev];
+    if (sm)
+        PFF_PROBED("k_relabel_jump_block", st, k_relabel_jump_block<<<1, 1024, RJ_SMEM, st>>>(fin, pits, np, hj, set));
+    else
+        PFF_PROBED("k_relabel_jump_block", st, k_relabel_jump_global<<<1, 1024, 0, st>>>(fin, pits, np, hj, set));
+    count_launch();
 }
 
 __global__ void __launch_bounds__(256) k_relabel_jump_coop(int32_t *fin, const int *__restrict__ pits, const int *np,
@@ -1284,8 +1385,10 @@ static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long lon
     const int N = g.N();
     if (!aprev) {
         const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + SAD_ROWS - 1) / SAD_ROWS);
-        { k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist, nblist, anext,
-                                                                     nanext); count_launch(); }
+        PFF_PROBED("k_saddle_p12_strip", st,
+                   k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist,
+                                                                              nblist, anext, nanext));
+        count_launch();
     } else {
         { k_saddle_p12_border<MODE><<<grid, 256, 0, st>>>(bid, isb, zp, saddle, z, g, aprev, naprev, anext, nanext,
                                                            blist, nblist); count_launch(); }
@@ -1653,7 +1756,7 @@ static int rr_iteration(const RRBufs &A, int par, bool first, cudaStream_t s, cu
     int32_t *fin = w.fin;
     cudaGraphConditionalHandle hj;
     PFF_TRY(rr_handle(s, &hj));
-    { k_relabel_jump_block<<<1, 1024, 0, s>>>(fin, plist, np, hj, 1); count_launch(); }
+    launch_relabel_jump_block(fin, plist, np, hj, 1, s);
     cudaGraph_t jbody = nullptr;
     PFF_TRY(rr_cond(s, hj, cudaGraphCondTypeIf, &jbody));
     PFF_CUDA(cudaStreamBeginCaptureToGraph(aux, jbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
@@ -2078,7 +2181,7 @@ static int reroute_host_loop(int32_t *bid, int32_t *rec, int32_t *rec_, int32_t 
             coop_relabel = nsm * (per < 4 ? per : 4);
         }
         int *plist = w.pits[par];
-        { k_relabel_jump_block<<<1, 1024, 0, st>>>(w.fin, plist, np, cudaGraphConditionalHandle{}, 0); count_launch(); }
+        launch_relabel_jump_block(w.fin, plist, np, cudaGraphConditionalHandle{}, 0, st);
         void *args[] = {&w.fin, &plist, &np, &flags};
         PFF_CUDA(cudaLaunchCooperativeKernel((void *)k_relabel_jump_coop, coop_relabel, 256, args, 0, st));
         count_launch();
@@ -2171,6 +2274,7 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
                                 int *n_outer_out, void *stream)
 {
     clear_error();
+    rj_prepare();
     PFF_TRY(check_grid(nx, ny, bound_mode, codes));
     if (!bid || !rec || !rec_ || !rec__ || !z || !z_prime || !is_border || !outlet || !basin_saddle ||
         !basin_saddlenode || !tag || !tag_) {
@@ -2245,6 +2349,7 @@ static RRKernelCounts g_async_kc[64];
 extern "C" int pff_reroute_flow_async(PFF_REROUTE_ARGS, int *ctl_out, void *stream)
 {
     clear_error();
+    rj_prepare();
     PFF_TRY(reroute_args_ok("pff_reroute_flow_async", bid, rec, rec_, rec__, z, z_prime, is_border, outlet,
                             basin_saddle, basin_saddlenode, tag, tag_, nx, ny, bound_mode, codes, workspace,
                             workspace_bytes));

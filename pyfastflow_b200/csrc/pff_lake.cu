@@ -642,6 +642,188 @@ __global__ void __launch_bounds__(128) k_saddle_p12_strip(const int32_t *__restr
     }
 }
 
+// Pass 1+2 with 4 columns per thread (modes 0-2, nx % 4 == 0, 16-byte aligned rows):
+// a warp walks a 128-column strip down SAD4_ROWS rows with 16-byte loads of the
+// labels and z, two rows of loads in flight.  A cell that cannot leave the domain
+// has all four links valid in these modes (edge links wrap in the periodic ones),
+// so every such cell takes the same path; edge-leaving cells only set z' = z.
+// Border cells collect in a per-warp shared buffer as in k_saddle_p12_strip.
+constexpr int SAD4_ROWS = 8;
+template <int MODE>
+__global__ void __launch_bounds__(128, 4) k_saddle_p12_strip4(const int32_t *__restrict__ bid, uint8_t *is_border,
+                                                              float *zp, long long *saddle, const float *__restrict__ z,
+                                                              Grid g, int *blist, int *nblist, int *alist, int *nalist)
+{
+    static_assert(MODE >= 0 && MODE <= 2, "custom codes take k_saddle_p12_strip");
+    __shared__ int buf[4][128 * SAD4_ROWS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int warp = blockIdx.x * 4 + wib;
+    const int nx = g.nx, ny = g.ny, nx4 = nx >> 2;
+    const int nstrips = (nx + 127) >> 7;
+    const int strip = warp % nstrips, band = warp / nstrips;
+    const int c0 = (strip << 7) + 4 * lane;
+    const int r0 = band * SAD4_ROWS;
+    if (r0 >= ny) return;
+    const int r1 = min(r0 + SAD4_ROWS, ny);
+    const bool incol = c0 < nx;
+    const int q0 = c0 >> 2;
+    const int4 *b4 = reinterpret_cast<const int4 *>(bid);
+    const float4 *z4 = reinterpret_cast<const float4 *>(z);
+    // halo columns at the strip edges (wrapped in periodic east-west)
+    const bool lhalo = incol && lane == 0 && (c0 > 0 || MODE == 1);
+    const bool rhalo = incol && (lane == 31 || c0 + 4 == nx) && (c0 + 4 < nx || MODE == 1);
+    const int lcol = c0 > 0 ? c0 - 1 : nx - 1, rcol = c0 + 4 < nx ? c0 + 4 : 0;
+    // row index of the row below rw (wrapped in periodic north-south; -1: none or past the band)
+    auto below = [&](int rw) -> int {
+        const int rb = rw + 1;
+        if (rb > r1) return -1;
+        return rb < ny ? rb : (MODE == 2 ? 0 : -1);
+    };
+    const int4 zi4 = make_int4(0, 0, 0, 0);
+    const float4 zf4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int4 bc = zi4, ba = zi4;
+    float4 zc = zf4, za = zf4;
+    int hbl = 0, hbr = 0;
+    float hzl = 0.f, hzr = 0.f;
+    if (incol) {
+        bc = b4[(size_t)r0 * nx4 + q0];
+        zc = z4[(size_t)r0 * nx4 + q0];
+        const int ra = r0 > 0 ? r0 - 1 : (MODE == 2 ? ny - 1 : -1);
+        if (ra >= 0) {
+            ba = b4[(size_t)ra * nx4 + q0];
+            za = z4[(size_t)ra * nx4 + q0];
+        }
+    }
+    if (lhalo) { hbl = bid[(size_t)r0 * nx + lcol]; hzl = z[(size_t)r0 * nx + lcol]; }
+    if (rhalo) { hbr = bid[(size_t)r0 * nx + rcol]; hzr = z[(size_t)r0 * nx + rcol]; }
+    int4 rb_[2];
+    float4 rz_[2];
+    int rbl[2], rbr[2];
+    float rzl[2], rzr[2];
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const int rl = below(r0 + p), rh = r0 + 1 + p;
+        rb_[p] = (incol && rl >= 0) ? b4[(size_t)rl * nx4 + q0] : zi4;
+        rz_[p] = (incol && rl >= 0) ? z4[(size_t)rl * nx4 + q0] : zf4;
+        rbl[p] = (lhalo && rh < r1) ? bid[(size_t)rh * nx + lcol] : 0;
+        rzl[p] = (lhalo && rh < r1) ? z[(size_t)rh * nx + lcol] : 0.f;
+        rbr[p] = (rhalo && rh < r1) ? bid[(size_t)rh * nx + rcol] : 0;
+        rzr[p] = (rhalo && rh < r1) ? z[(size_t)rh * nx + rcol] : 0.f;
+    }
+    int nb = 0;  // border cells buffered by this warp
+    const long long iv = invalid_key();
+    for (int rb0 = r0; rb0 < r1; rb0 += 2) {
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int rw = rb0 + p;
+            if (rw >= r1) break;
+            const int4 bb = rb_[p];
+            const float4 zb = rz_[p];
+            const int nbl = rbl[p], nbr = rbr[p];
+            const float nzl = rzl[p], nzr = rzr[p];
+            {
+                const int rl = below(rw + 2), rh = rw + 3;
+                rb_[p] = (incol && rl >= 0) ? b4[(size_t)rl * nx4 + q0] : zi4;
+                rz_[p] = (incol && rl >= 0) ? z4[(size_t)rl * nx4 + q0] : zf4;
+                rbl[p] = (lhalo && rh < r1) ? bid[(size_t)rh * nx + lcol] : 0;
+                rzl[p] = (lhalo && rh < r1) ? z[(size_t)rh * nx + lcol] : 0.f;
+                rbr[p] = (rhalo && rh < r1) ? bid[(size_t)rh * nx + rcol] : 0;
+                rzr[p] = (rhalo && rh < r1) ? z[(size_t)rh * nx + rcol] : 0.f;
+            }
+            int bl = __shfl_up_sync(0xffffffffu, bc.w, 1), br = __shfl_down_sync(0xffffffffu, bc.x, 1);
+            float zl = __shfl_up_sync(0xffffffffu, zc.w, 1), zr = __shfl_down_sync(0xffffffffu, zc.x, 1);
+            if (lhalo) { bl = hbl; zl = hzl; }
+            if (rhalo) { br = hbr; zr = hzr; }
+            int listed[4] = {0, 0, 0, 0};
+            if (incol) {
+                const int bcv[4] = {bc.x, bc.y, bc.z, bc.w}, bav[4] = {ba.x, ba.y, ba.z, ba.w},
+                          bbv[4] = {bb.x, bb.y, bb.z, bb.w};
+                const float zcv[4] = {zc.x, zc.y, zc.z, zc.w}, zav[4] = {za.x, za.y, za.z, za.w},
+                            zbv[4] = {zb.x, zb.y, zb.z, zb.w};
+                const bool rowleave = MODE != 2 && (rw == 0 || rw == ny - 1);
+                float zpo[4];
+                unsigned char isb[4];
+                bool wb[4];
+                const int i0 = rw * nx + c0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int col = c0 + k;
+                    const bool leave = rowleave || (MODE != 1 && (col == 0 || col == nx - 1));
+                    const int bi = bcv[k];
+                    const float zi = zcv[k];
+                    // neighbours: top, left, right, bottom (all valid for a cell that cannot leave)
+                    const int bn[4] = {bav[k], k > 0 ? bcv[k - 1] : bl, k < 3 ? bcv[k + 1] : br, bbv[k]};
+                    const float zn[4] = {zav[k], k > 0 ? zcv[k - 1] : zl, k < 3 ? zcv[k + 1] : zr, zbv[k]};
+                    bool border = false;
+                    float zmin = 1e9f;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                        if (bn[m] != bi) { border = true; zmin = fminf(zmin, zn[m]); }
+                    const float zpi = border ? fmaxf(zi, zmin) : 1e9f;
+                    zpo[k] = leave ? zi : zpi;
+                    isb[k] = border;
+                    wb[k] = !leave;
+                    if (!leave && border) {
+                        long long res = iv;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            if (bn[m] == bi) continue;
+                            const long long cand = pack_key(zpi, bn[m]);
+                            res = cand < res ? cand : res;
+                        }
+                        if (res != iv) atomicMin(saddle + bi, res);
+                        listed[k] = bi != 0 ? 2 : 1;
+                    }
+                }
+                reinterpret_cast<float4 *>(zp)[(size_t)rw * nx4 + q0] = make_float4(zpo[0], zpo[1], zpo[2], zpo[3]);
+                if (wb[0] && wb[1] && wb[2] && wb[3]) {
+                    reinterpret_cast<uchar4 *>(is_border)[(size_t)rw * nx4 + q0] = make_uchar4(isb[0], isb[1], isb[2], isb[3]);
+                } else {  // a cell that can leave keeps its is_border (lakeflow.py:133-135)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (wb[k]) is_border[i0 + k] = isb[k];
+                }
+            }
+            // every border cell, the pit-basin ones marked by the sign bit
+            const int irow = rw * nx + c0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const bool has = listed[k] != 0;
+                const unsigned m = __ballot_sync(0xffffffffu, has);
+                if (has)
+                    buf[wib][nb + __popc(m & ((1u << lane) - 1u))] =
+                        listed[k] == 2 ? ((irow + k) | (int)0x80000000) : (irow + k);
+                nb += __popc(m);
+            }
+            ba = bc; za = zc;
+            bc = bb; zc = zb;
+            hbl = nbl; hzl = nzl; hbr = nbr; hzr = nzr;
+        }
+    }
+    __syncwarp();
+    int npit = 0;
+    for (int k = lane; k < nb; k += 32) npit += buf[wib][k] < 0;
+    npit = __reduce_add_sync(0xffffffffu, npit);
+    int bp = 0, bq = 0;  // bases in blist and alist
+    if (lane == 0) {
+        if (npit) bp = atomicAdd(nblist, npit);
+        if (alist && nb) bq = atomicAdd(nalist, nb);
+    }
+    bp = __shfl_sync(0xffffffffu, bp, 0);
+    bq = __shfl_sync(0xffffffffu, bq, 0);
+    int run = 0;
+    for (int k0 = 0; k0 < nb; k0 += 32) {
+        const int k = k0 + lane;
+        const int v = k < nb ? buf[wib][k] : 0;
+        const bool pit = k < nb && v < 0;
+        const int i = v & 0x7FFFFFFF;
+        if (alist && k < nb) alist[bq + k] = i;
+        const unsigned m = __ballot_sync(0xffffffffu, pit);
+        if (pit) blist[bp + run + __popc(m & ((1u << lane) - 1u))] = i;
+        run += __popc(m);
+    }
+}
+
 // Pass 1+2 of a later outer iteration over the border cells of the previous one.
 // Labels change between outer iterations only by merging basins (b -> fin(b)), so
 // a cell whose neighbours all shared its label still does, keeps is_border = 0
@@ -989,9 +1171,8 @@ __global__ void k_relabel_init(int32_t *fin, const int32_t *__restrict__ bid, co
 // Inside the reroute graph the block kernel also sets a conditional handle, so the
 // cooperative launch (whose launch alone costs about 10 us) runs only for long lists.
 constexpr int RJ_BLOCK = 16384;
-// The one-CTA jump in global memory: the fallback of the shared-memory version below.
-__global__ void __launch_bounds__(1024) k_relabel_jump_global(int32_t *fin, const int *__restrict__ pits,
-                                                              const int *np, cudaGraphConditionalHandle hj, int set)
+__global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const int *__restrict__ pits, const int *np,
+                                                            cudaGraphConditionalHandle hj, int set)
 {
     const int n = *np;
     if (set && threadIdx.x == 0) cudaGraphSetConditional(hj, n > RJ_BLOCK ? 1u : 0u);
@@ -1007,97 +1188,10 @@ __global__ void __launch_bounds__(1024) k_relabel_jump_global(int32_t *fin, cons
         if (!__syncthreads_or(ch)) break;
     }
 }
-
-// The same jump with the chains in shared memory.  A target basin is 0 (the outlet
-// basin) or, when the labels are current, a basin of the pit list itself; so the
-// chain is followed over list slots: fin[b] briefly holds b's slot, each pit's target
-// slot is looked up there, and the jumping runs on slots in shared memory (a round
-// costs shared-memory latency instead of two dependent global loads).  A target that
-// is not in the list (labels not current, as after a receiver cycle) restores fin and
-// runs the global-memory rounds instead, so the result is the same in every case.
-constexpr size_t RJ_SMEM = 2 * RJ_BLOCK * sizeof(int);
-__global__ void __launch_bounds__(1024) k_relabel_jump_block(int32_t *fin, const int *__restrict__ pits,
-                                                             const int *np, cudaGraphConditionalHandle hj, int set)
-{
-    extern __shared__ int rj_sm[];
-    int *tgt = rj_sm, *t = rj_sm + RJ_BLOCK;
-    __shared__ int bad;
-    const int n = *np;
-    if (set && threadIdx.x == 0) cudaGraphSetConditional(hj, n > RJ_BLOCK ? 1u : 0u);
-    if (n > RJ_BLOCK) return;
-    if (threadIdx.x == 0) bad = 0;
-    for (int k = threadIdx.x; k < n; k += 1024) tgt[k] = fin[pits[k] + 1];
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += 1024) fin[pits[k] + 1] = k;
-    __syncthreads();  // the block's own global writes are visible to it after the barrier
-    for (int k = threadIdx.x; k < n; k += 1024) {
-        const int x = tgt[k];
-        int sl = -1;
-        if (x != 0) {
-            sl = x > 0 ? fin[x] : -1;
-            if ((unsigned)sl >= (unsigned)n || pits[sl] + 1 != x) {
-                sl = k;
-                bad = 1;
-            }
-        }
-        t[k] = sl;
-    }
-    __syncthreads();
-    if (bad) {  // restore the targets and take the global-memory rounds
-        for (int k = threadIdx.x; k < n; k += 1024) fin[pits[k] + 1] = tgt[k];
-        __syncthreads();
-        for (int r = 0; r < 32; ++r) {
-            bool ch = false;
-            for (int k = threadIdx.x; k < n; k += 1024) {
-                const int b = pits[k] + 1;
-                const int x = fin[b];
-                const int y = fin[x];
-                if (y != x) { fin[b] = y; ch = true; }
-            }
-            if (!__syncthreads_or(ch)) break;
-        }
-        return;
-    }
-    for (int r = 0; r < 32; ++r) {
-        bool ch = false;
-        for (int k = threadIdx.x; k < n; k += 1024) {
-            const int x = t[k];
-            if (x >= 0) {
-                const int y = t[x];
-                if (y != x) { t[k] = y; ch = true; }
-            }
-        }
-        if (!__syncthreads_or(ch)) break;
-    }
-    for (int k = threadIdx.x; k < n; k += 1024) {
-        const int x = t[k];
-        fin[pits[k] + 1] = x < 0 ? 0 : pits[x] + 1;
-    }
-}
-
-// The shared-memory jump needs more than the default 48 KB of dynamic shared memory;
-// the attribute (not a stream operation) is set once per device by the reroute's entry
-// points before they launch anything.  Without it the global-memory kernel runs.
-static bool g_rj_smem[64];
-static void rj_prepare()
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || g_rj_smem[dev]) return;
-    if (cudaFuncSetAttribute(k_relabel_jump_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RJ_SMEM) ==
-        cudaSuccess)
-        g_rj_smem[dev] = true;
-    else
-        cudaGetLastError();
-}
 static void launch_relabel_jump_block(int32_t *fin, const int *pits, const int *np, cudaGraphConditionalHandle hj,
                                       int set, cudaStream_t st)
 {
-    int dev = 0;
-    const bool sm = cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && g_rj_smem[dev];
-    if (sm)
-        PFF_PROBED("k_relabel_jump_block", st, k_relabel_jump_block<<<1, 1024, RJ_SMEM, st>>>(fin, pits, np, hj, set));
-    else
-        PFF_PROBED("k_relabel_jump_block", st, k_relabel_jump_global<<<1, 1024, 0, st>>>(fin, pits, np, hj, set));
+    PFF_PROBED("k_relabel_jump_block", st, k_relabel_jump_block<<<1, 1024, 0, st>>>(fin, pits, np, hj, set));
     count_launch();
 }
 
@@ -1383,7 +1477,17 @@ static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long lon
                            int *nanext, int grid, cudaStream_t st)
 {
     const int N = g.N();
-    if (!aprev) {
+    const bool vec = g.nx % 4 == 0 && ((uintptr_t)bid % 16) == 0 && ((uintptr_t)z % 16) == 0 &&
+                     ((uintptr_t)zp % 16) == 0 && ((uintptr_t)isb % 4) == 0;
+    if (!aprev && MODE != 3 && vec) {
+        if constexpr (MODE != 3) {
+            const long long warps = (long long)((g.nx + 127) / 128) * ((g.ny + SAD4_ROWS - 1) / SAD4_ROWS);
+            PFF_PROBED("k_saddle_p12_strip", st,
+                       k_saddle_p12_strip4<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist,
+                                                                                   nblist, anext, nanext));
+            count_launch();
+        }
+    } else if (!aprev) {
         const long long warps = (long long)((g.nx + 31) / 32) * ((g.ny + SAD_ROWS - 1) / SAD_ROWS);
         PFF_PROBED("k_saddle_p12_strip", st,
                    k_saddle_p12_strip<MODE><<<div_up(warps, 4), 128, 0, st>>>(bid, isb, zp, saddle, z, g, blist,
@@ -2274,7 +2378,6 @@ extern "C" int pff_reroute_flow(int32_t *bid, int32_t *rec, int32_t *rec_, int32
                                 int *n_outer_out, void *stream)
 {
     clear_error();
-    rj_prepare();
     PFF_TRY(check_grid(nx, ny, bound_mode, codes));
     if (!bid || !rec || !rec_ || !rec__ || !z || !z_prime || !is_border || !outlet || !basin_saddle ||
         !basin_saddlenode || !tag || !tag_) {
@@ -2349,7 +2452,6 @@ static RRKernelCounts g_async_kc[64];
 extern "C" int pff_reroute_flow_async(PFF_REROUTE_ARGS, int *ctl_out, void *stream)
 {
     clear_error();
-    rj_prepare();
     PFF_TRY(reroute_args_ok("pff_reroute_flow_async", bid, rec, rec_, rec__, z, z_prime, is_border, outlet,
                             basin_saddle, basin_saddlenode, tag, tag_, nx, ny, bound_mode, codes, workspace,
                             workspace_bytes));

@@ -374,7 +374,7 @@ def main():
     wh = torch.from_numpy(w).pin_memory()
     qh = torch.empty(n * n, dtype=torch.float32).pin_memory()
     ch = torch.empty(n * n, dtype=torch.int32).pin_memory()
-    e2e_steps = max(2, min(args.steps, 8))
+    e2e_steps = max(2, args.steps)  # as many DEMs as timed steps: the first copy in and the last copy out do not overlap
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # one DEM per step through FlowRouter.route_many: every step copies its DEM and
@@ -395,6 +395,30 @@ def main():
         torch.distributed.all_reduce(t_e, op=torch.distributed.ReduceOp.MAX)
     e2e_v = world * n * n * e2e_steps / (float(t_e.item()) * 1e-3) / 1e6
 
+    # the host link alone: the same per-step copies (DEM and weights in, Q and counts out, on two
+    # copy streams at once) without the routing, the bound the end-to-end figure can reach
+    cs_in, cs_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    zd_c, wd_c = torch.empty(n * n, dtype=torch.float32, device=dev), torch.empty(n * n, dtype=torch.float32, device=dev)
+    qd_c, cd_c = torch.empty(n * n, dtype=torch.float32, device=dev), torch.empty(n * n, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    cs_in.wait_event(c0)
+    cs_out.wait_event(c0)
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(cs_in):
+            zd_c.copy_(zh, non_blocking=True)
+            wd_c.copy_(wh, non_blocking=True)
+        with torch.cuda.stream(cs_out):
+            qh.copy_(qd_c, non_blocking=True)
+            ch.copy_(cd_c, non_blocking=True)
+    torch.cuda.current_stream().wait_stream(cs_in)
+    torch.cuda.current_stream().wait_stream(cs_out)
+    c1.record()
+    torch.cuda.synchronize()
+    copy_ms = c0.elapsed_time(c1) / e2e_steps
+    del zd_c, wd_c, qd_c, cd_c
+
     out = {"metric": METRIC, "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded spectral DEM + Gaussian pits)",
@@ -404,7 +428,9 @@ def main():
            "gpu_launches": int(launches),
            "e2e": {"value": e2e_v, "unit": "Mcells/s", "h2d_bytes_per_step": 8 * n * n,
                    "d2h_bytes_per_step": 8 * n * n, "steps": e2e_steps,
-                   "api": "FlowRouter.route_many (copies of neighbouring steps overlap the routing)"}}
+                   "api": "FlowRouter.route_many (copies of neighbouring steps overlap the routing)",
+                   "copies_alone_ms_per_step": copy_ms,
+                   "copies_alone_mcells": n * n / (copy_ms * 1e-3) / 1e6}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # bounded: one run of the whole chain on the same DEM and weights (about 15 s
         # on 16 host cores), no warm-up (the restatement is compiled C: nothing to JIT)

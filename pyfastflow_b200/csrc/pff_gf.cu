@@ -331,6 +331,23 @@ __global__ void __launch_bounds__(DF_THREADS) k_diffuse_fused(const float *__res
 #pragma unroll
     for (int sw = 1; sw <= H; ++sw) {
         const int bw = RX - 2 * sw, bh = RY - 2 * sw;
+        if (inner) {  // every cell inside the grid, off its edges: summation order top, left, right, bottom
+            for (int t = threadIdx.x; t < bw * bh; t += blockDim.x) {
+                const int i = (sw + t / bw) * RX + sw + t % bw;
+                const int u = i - RX, l = i - 1, rt = i + 1, d = i + RX;
+                float acc = prec_dx2;
+                acc = df_add(acc, w3[u], qc[u]);
+                acc = df_add(acc, w2[l], qc[l]);
+                acc = df_add(acc, w1[rt], qc[rt]);
+                acc = df_add(acc, w0[d], qc[d]);
+                qn[i] = acc;
+            }
+            __syncthreads();
+            float *tq = qc;
+            qc = qn;
+            qn = tq;
+            continue;
+        }
         for (int t = threadIdx.x; t < bw * bh; t += blockDim.x) {
             const int i = (sw + t / bw) * RX + sw + t % bw;
             const unsigned char f = fl[i];

@@ -374,16 +374,22 @@ __device__ void tile_terminal_one(const int32_t *__restrict__ rec, int32_t *J, i
         ext[c] = e;
     }
     __syncthreads();
-    // at most ceil(log2 2048) = 11 rounds for any acyclic in-tile path
+    // at most ceil(log2 2048) = 11 rounds for any acyclic in-tile path.  A thread reads
+    // all its cells' pointers, then all the pointers they point to, then stores: the
+    // shared-memory round trips overlap (one interleaving of the same concurrent updates)
     for (int round = 0; round < 12; ++round) {
         bool ch = false;
+        int q[TILE_PER_THREAD], qq[TILE_PER_THREAD];
 #pragma unroll
-        for (int k = 0; k < TILE_PER_THREAD; ++k) {
-            const int c = threadIdx.x + k * TILE_THREADS;
-            const int q = p[c];
-            const int qq = p[q];
-            if (qq != q) { p[c] = qq; ch = true; }
-        }
+        for (int k = 0; k < TILE_PER_THREAD; ++k) q[k] = p[threadIdx.x + k * TILE_THREADS];
+#pragma unroll
+        for (int k = 0; k < TILE_PER_THREAD; ++k) qq[k] = p[q[k]];
+#pragma unroll
+        for (int k = 0; k < TILE_PER_THREAD; ++k)
+            if (qq[k] != q[k]) {
+                p[threadIdx.x + k * TILE_THREADS] = qq[k];
+                ch = true;
+            }
         if (!__syncthreads_or(ch)) break;
     }
     bool nonlocal = false;

@@ -1,6 +1,7 @@
 """The bench's clock sampler against a fake NVML (no GPU, read-only queries):
 samples are taken while the timed region runs, the clock-event reason bits map to
-the names a run is judged by, and a failing query is reported, not swallowed."""
+the throttle-reason names that mark a measurement as slowed down, and a failing
+query is reported, not swallowed."""
 import sys
 import time
 import types

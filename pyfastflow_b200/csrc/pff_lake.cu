@@ -1460,6 +1460,19 @@ template <int MODE>
 static void l_tile_terminal_list(const int32_t *rec, int32_t *J, int32_t *R, int *info, const Grid &g,
                                  const int *tiles, const int *ntiles, int grid, cudaStream_t st)
 {
+    // the CTAs loop over the list: no more of them than fit on the GPU at once, so that
+    // none waits for a second wave with its share of the tiles
+    static int resident[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+        if (!resident[dev]) {
+            int per = 0, nsm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tile_terminal<MODE>, TILE_THREADS, 0);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            resident[dev] = per > 0 && nsm > 0 ? per * nsm : -1;
+        }
+        if (resident[dev] > 0) grid = std::min(grid, resident[dev]);
+    }
     PFF_PROBED("k_tile_terminal<list>", st,
                k_tile_terminal<MODE><<<grid, TILE_THREADS, 0, st>>>(rec, J, R, nullptr, info, g, tiles, ntiles));
     count_launch();

@@ -455,6 +455,58 @@ __global__ void __launch_bounds__(256) k_labels_final(const int32_t *__restrict_
     bid[i] = can_leave_i<MODE>(g, root) ? 0 : root + 1;
 }
 
+// Exact quotient and remainder of n / d for 0 <= n < 2^31 and d >= 2 without the
+// integer divide sequence: q = umulhi(n, m) with m = floor(2^32 / d) is floor(n / d)
+// or one less (n m / 2^32 > n / d - n / 2^32 > n / d - 1), and one correction of the
+// remainder fixes it.
+__device__ __forceinline__ void divmod_nx(int n, int d, unsigned m, int &q, int &r)
+{
+    q = (int)__umulhi((unsigned)n, m);
+    r = n - q * d;
+    if (r >= d) { ++q; r -= d; }
+}
+
+// k_labels_final on 4 cells per thread (modes 0-2, nx % 4 == 0): 16-byte loads and
+// stores, the gathers of the 4 cells in flight together, and the roots' rows and
+// columns without integer division.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_labels_final4(const int32_t *__restrict__ J, const int32_t *__restrict__ R,
+                                                       int32_t *bid, Grid g, const int32_t *__restrict__ rec,
+                                                       int *unresolved, unsigned mnx)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (4 * q >= g.N()) return;
+    const int4 j = reinterpret_cast<const int4 *>(J)[q];
+    const int rt[4] = {R[j.x], R[j.y], R[j.z], R[j.w]};
+    const int rr[4] = {rec[rt[0]], rec[rt[1]], rec[rt[2]], rec[rt[3]]};
+    int lab[4];
+    bool cyc = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        cyc |= rr[k] != rt[k];  // a receiver cycle: labels need the general path
+        int row, col;
+        divmod_nx(rt[k], g.nx, mnx, row, col);
+        lab[k] = can_leave<MODE>(g, rt[k], row, col) ? 0 : rt[k] + 1;
+    }
+    reinterpret_cast<int4 *>(bid)[q] = make_int4(lab[0], lab[1], lab[2], lab[3]);
+    if (cyc) *unresolved = 1;
+}
+
+// k_basin_init on 4 cells of one row per thread (modes 0-2, nx % 4 == 0)
+template <int MODE>
+__global__ void k_basin_init4(int32_t *bid, Grid g, const int *guard, unsigned mnx)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = 4 * q;
+    if (i0 >= g.N() || (guard && *guard == 0)) return;
+    int row, col;
+    divmod_nx(i0, g.nx, mnx, row, col);
+    int lab[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) lab[k] = can_leave<MODE>(g, i0 + k, row, col + k) ? 0 : i0 + k + 1;
+    reinterpret_cast<int4 *>(bid)[q] = make_int4(lab[0], lab[1], lab[2], lab[3]);
+}
+
 // ---- list-driven saddle passes ---------------------------------------------------
 
 // reset the basin entries of a pit list (basin = pit + 1) and entry 0
@@ -1430,6 +1482,11 @@ static void l_count_pits(const int32_t *rec, const Grid &g, int *count, int *lis
 template <int MODE>
 static void l_basin_init(int32_t *bid, const Grid &g, cudaStream_t st)
 {
+    if (MODE != 3 && g.nx % 4 == 0 && ((uintptr_t)bid % 16) == 0) {
+        const unsigned m = (unsigned)(0x100000000ull / (unsigned long long)g.nx);
+        { k_basin_init4<MODE == 3 ? 0 : MODE><<<div_up(g.N() / 4, 256), 256, 0, st>>>(bid, g, nullptr, m); count_launch(); }
+        return;
+    }
     { k_basin_init<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(bid, g, nullptr); count_launch(); }
 }
 template <int MODE>
@@ -1481,6 +1538,12 @@ template <int MODE>
 static void l_labels_final(const int32_t *J, const int32_t *R, int32_t *bid, const Grid &g, const int32_t *rec,
                            int *unresolved, cudaStream_t st)
 {
+    if (MODE != 3 && g.nx % 4 == 0 && ((uintptr_t)J % 16) == 0 && ((uintptr_t)bid % 16) == 0) {
+        const unsigned m = (unsigned)(0x100000000ull / (unsigned long long)g.nx);
+        { k_labels_final4<MODE == 3 ? 0 : MODE><<<div_up(g.N() / 4, 256), 256, 0, st>>>(J, R, bid, g, rec, unresolved, m);
+          count_launch(); }
+        return;
+    }
     { k_labels_final<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(J, R, bid, g, rec, unresolved); count_launch(); }
 }
 template <int MODE>
@@ -1526,6 +1589,11 @@ static void l_saddle_lists(const int32_t *bid, uint8_t *isb, float *zp, long lon
 template <int MODE>
 static void l_basin_init_if(int32_t *bid, const Grid &g, const int *guard, cudaStream_t st)
 {
+    if (MODE != 3 && g.nx % 4 == 0 && ((uintptr_t)bid % 16) == 0) {
+        const unsigned m = (unsigned)(0x100000000ull / (unsigned long long)g.nx);
+        { k_basin_init4<MODE == 3 ? 0 : MODE><<<div_up(g.N() / 4, 256), 256, 0, st>>>(bid, g, guard, m); count_launch(); }
+        return;
+    }
     { k_basin_init<MODE><<<div_up(g.N(), 256), 256, 0, st>>>(bid, g, guard); count_launch(); }
 }
 

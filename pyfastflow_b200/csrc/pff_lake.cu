@@ -456,9 +456,10 @@ __global__ void __launch_bounds__(256) k_labels_final(const int32_t *__restrict_
 }
 
 // Exact quotient and remainder of n / d for 0 <= n < 2^31 and d >= 2 without the
-// integer divide sequence: q = umulhi(n, m) with m = floor(2^32 / d) is floor(n / d)
-// or one less (n m / 2^32 > n / d - n / 2^32 > n / d - 1), and one correction of the
-// remainder fixes it.
+// integer divide sequence: with m = floor(2^32 / d) or m = floor((2^32 - 1) / d) (one
+// less only when d divides 2^32), q = umulhi(n, m) is floor(n / d) or one less
+// (n m / 2^32 > n / d - 2 n / 2^32 > n / d - 1), and one correction of the remainder
+// fixes it.
 __device__ __forceinline__ void divmod_nx(int n, int d, unsigned m, int &q, int &r)
 {
     q = (int)__umulhi((unsigned)n, m);
@@ -896,6 +897,7 @@ __global__ void __launch_bounds__(256) k_saddle_p12_border(const int32_t *__rest
     const int n = *naprev;
     const int stride = gridDim.x * 256;
     const int trips = (n + stride - 1) / stride;
+    const unsigned mnx = 0xffffffffu / (unsigned)g.nx;  // divmod_nx's multiplier (one division per thread)
     for (int k = 0; k < trips; ++k) {
         const int idx = k * stride + blockIdx.x * 256 + threadIdx.x;
         int code = 0, i = -1, bi = 0;
@@ -903,7 +905,8 @@ __global__ void __launch_bounds__(256) k_saddle_p12_border(const int32_t *__rest
         bool has = false;
         if (idx < n) {
             i = aprev[idx];
-            const int row = i / g.nx, col = i - row * g.nx;
+            int row, col;
+            divmod_nx(i, g.nx, mnx, row, col);
             int jn[4], bn[4];
             float zn[4];
             neighbours4<MODE>(g, i, row, col, jn);
@@ -928,6 +931,7 @@ __global__ void __launch_bounds__(256) k_saddle_p3_list(const int32_t *__restric
                                                         const int *__restrict__ blist, const int *nblist)
 {
     const int n = *nblist;
+    const unsigned mnx = 0xffffffffu / (unsigned)g.nx;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int i = blist[k];
         const int bi = bid[i];
@@ -935,10 +939,12 @@ __global__ void __launch_bounds__(256) k_saddle_p3_list(const int32_t *__restric
         const float tz = key_value(s);
         const int tb = key_index(s);
         const float zpi = zp[i];
+        int row, col;
+        divmod_nx(i, g.nx, mnx, row, col);
         bool here = false;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int j = neighbour_i<MODE>(g, i, q);
+            const int j = neighbour<MODE>(g, i, row, col, q);
             if (j != -1 && bid[j] == tb && zpi == tz) here = true;
         }
         if (here) atomicMax(snode + bi, i);
@@ -952,6 +958,7 @@ __global__ void k_saddle_p4_list(const int32_t *__restrict__ bid, const long lon
 {
     const int n = *np;
     const long long iv = invalid_key();
+    const unsigned mnx = 0xffffffffu / (unsigned)g.nx;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int b = pits[k] + 1;
         if (b >= g.N() || saddle[b] == iv) continue;  // the reference's pass 4 loop stops at N-1
@@ -959,9 +966,11 @@ __global__ void k_saddle_p4_list(const int32_t *__restrict__ bid, const long lon
         if (node < 0) continue;
         float tz = 1e9f;
         int r = -1;
+        int row, col;
+        divmod_nx(node, g.nx, mnx, row, col);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int j = neighbour_i<MODE>(g, node, q);
+            const int j = neighbour<MODE>(g, node, row, col, q);
             if (j == -1) continue;
             const float zj = z[j];
             if (bid[j] != b && tz > zj) { tz = zj; r = j; }
@@ -1113,6 +1122,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_carve_walk(const int32_t *__re
             walk_segment(segs[k], rec0, rec, tag, tag_, nx, dirty);
         return;
     }
+    const unsigned mnx = 0xffffffffu / (unsigned)nx;  // divmod_nx's multiplier
     for (int k = blockIdx.x; k < n; k += gridDim.x) {
     const int s0 = segs[k];
     static_assert(TILE_W == 64, "local index = row * 64 + column");
@@ -1126,7 +1136,8 @@ __global__ void __launch_bounds__(WALK_THREADS) k_carve_walk(const int32_t *__re
         int v = q;  // cells past the grid edge: terminal, never reached
         if (lr < h && lc < w) {
             const int r = rec0[(r0 + lr) * nx + c0 + lc];
-            const int rr = r / nx, rc = r - rr * nx;
+            int rr, rc;
+            divmod_nx(r, nx, mnx, rr, rc);
             v = (rr / TILE_H == ty && rc / TILE_W == tx) ? (((rr - r0) << 6) | (rc - c0)) : ~r;
         }
         nl[q] = v;

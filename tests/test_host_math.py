@@ -5,8 +5,9 @@ like the GPU's __fdiv_rn / __fmul_rn):
 * receivers (csrc/pff_core.cu, rcv_off_fast): a drop d < dmax whose quotient by dx
   rounds to the same float32 as dmax's is never below RN(dmax * (1 - 2^-21)), so
   directions under that bound can be skipped when looking for a tie;
-* labels (csrc/pff_lake.cu, divmod_nx): umulhi(n, floor(2^32 / d)) is floor(n / d)
-  or one less for 0 <= n < 2^31, and one correction of the remainder makes it exact;
+* labels and list passes (csrc/pff_lake.cu, divmod_nx): umulhi(n, m) with
+  m = floor(2^32 / d) or floor((2^32 - 1) / d) is floor(n / d) or one less for
+  0 <= n < 2^31, and one correction of the remainder makes it exact;
 * the exact-division range (csrc/pff_div.cuh, make_divc) keeps the numerator and the
   quotient inside [2^-100, 2^100].
 """
@@ -40,8 +41,7 @@ def test_divmod_by_multiply_high():
     rng = np.random.default_rng(5)
     ds = np.concatenate([np.arange(2, 70), [127, 128, 129, 1000, 1024, 2047, 2048, 4095, 4096, 4097, 65535, 65536,
                                             (1 << 20) + 7, (1 << 29) + 1], rng.integers(2, 1 << 30, 200)])
-    for d in ds.tolist():
-        m = (1 << 32) // d
+    for d, m in [(d, (1 << 32) // d) for d in ds.tolist()] + [(d, ((1 << 32) - 1) // d) for d in ds.tolist()]:
         n = np.concatenate([np.arange(0, 3 * d if d < 5000 else 5000, dtype=np.int64),
                             rng.integers(0, 1 << 31, 20000), [(1 << 31) - 1, (1 << 31) - d, ((1 << 31) // d) * d - 1]])
         n = n[(n >= 0) & (n < (1 << 31))].astype(np.uint64)
